@@ -1,0 +1,428 @@
+// ab_backproject.cu -- voxel-driven cone-beam backprojection, all views in
+// one launch.
+//
+// Replaces backproject_CB_voltex<float,float>
+// (src/aprict/data/cusrc/CB_backproject.cu:952-1027; per-voxel body
+// _backproject_CB_getval :313-733) and the host loop that launches it once per
+// 10 views with the 640-byte proj_chunk_spec_maxlen10 passed by value
+// (src/aprict/cb/flatpanel.py:1192-1278).
+//
+// B200 layout: a warp covers 32 consecutive voxels along the volume's fastest
+// axis, so the final read-modify-write of the volume is one coalesced 128-byte
+// line per warp, and for circular scans the 32 voxel centres project onto one
+// detector column -- the projection gathers of a warp fall into 2-3 lines.
+// Each thread carries XB voxels along the slowest axis (independent
+// accumulators for ILP). Per-view coefficients (ab_bpview) are derived once per
+// CTA into shared memory and read as uniform broadcasts; the volume is read and
+// written exactly once per call instead of once per 10 views.
+#include <cuda_runtime.h>
+
+#include "ab_bpview.cuh"
+#include "ab_host.h"
+
+namespace {
+
+constexpr int kThreads = 256;  // 32 (fast axis) x 8 (middle axis)
+constexpr int kChunk = 128;    // views per shared-memory chunk
+constexpr int kXB = 4;         // voxels per thread along the slowest axis
+
+struct BPParams {
+    const aprict_proj_spec *specs;
+    uint32_t n_views, nu, nv;
+    ab_pstrides ps;
+    const float *projs;
+    float *vol;
+    const float *mult;
+    int n[3];          // volume shape (x, y, z)
+    int64_t vs[3];     // element strides (x, y, z)
+    float voxwid;
+    float c0[3];       // volume centre (world)
+    // config
+    int mask;
+    float mask_r2;
+    int all_ones;
+    float sep;
+    int pL, pV;
+    float val;
+    int ssx, ssy, ssz;
+    uint32_t *status;
+};
+
+// Pixel value with the reference's zero-order rule (get_zero_interp,
+// CB_backproject.cu:256-271): index floor(f + 0.5). When f + 0.5 lies within
+// kRefine of an integer the FP32 estimate cannot be trusted to pick the same
+// pixel as an exact evaluation, so the index is recomputed in FP64.
+constexpr float kRefine = 2e-3f;
+
+__device__ __forceinline__ bool near_half(float f) {
+    const float g = f + 0.5f;
+    return fabsf(g - rintf(g)) < kRefine;
+}
+
+__device__ __forceinline__ float fetch_nearest(const BPParams &P, int view, float fu, float fv, const float xw[3]) {
+    if (near_half(fu) || near_half(fv)) {
+        double du, dv;
+        const aprict_proj_spec sp = P.specs[view];
+        ab_project_point_d(sp, ab_d3{(double)xw[0], (double)xw[1], (double)xw[2]}, du, dv);
+        const int iu = (int)floor(du + 0.5), iv = (int)floor(dv + 0.5);
+        if (iu < 0 || iu >= (int)P.nu || iv < 0 || iv >= (int)P.nv) return 0.f;
+        return __ldg(P.projs + (int64_t)view * P.ps.view + (int64_t)iu * P.ps.u + (int64_t)iv * P.ps.v);
+    }
+    const float gu = floorf(fu + 0.5f), gv = floorf(fv + 0.5f);
+    if (!(gu >= 0.f && gu < (float)P.nu && gv >= 0.f && gv < (float)P.nv)) return 0.f;
+    return __ldg(P.projs + (int64_t)view * P.ps.view + (int64_t)gu * P.ps.u + (int64_t)gv * P.ps.v);
+}
+
+// Bilinear rule of get_bilinear_interp (CB_backproject.cu:221-254), same
+// operation order.
+__device__ __forceinline__ float fetch_bilinear(const BPParams &P, int view, float fu, float fv) {
+    if (fu <= -1.f || fv <= -1.f || fu >= (float)P.nu || fv >= (float)P.nv) return 0.f;
+    const int i0 = (int)floorf(fu), j0 = (int)floorf(fv);
+    const float fx = fu - (float)i0, fy = fv - (float)j0;
+    const float *base = P.projs + (int64_t)view * P.ps.view;
+    auto get = [&](int i, int j) -> float {
+        if (i < 0 || i >= (int)P.nu || j < 0 || j >= (int)P.nv) return 0.f;
+        return __ldg(base + (int64_t)i * P.ps.u + (int64_t)j * P.ps.v);
+    };
+    const float v00 = get(i0, j0), v01 = get(i0, j0 + 1), v10 = get(i0 + 1, j0), v11 = get(i0 + 1, j0 + 1);
+    const float t1 = v00 * (1.f - fx) + v10 * fx;
+    const float t2 = v01 * (1.f - fx) + v11 * fx;
+    return t1 * (1.f - fy) + t2 * fy;
+}
+
+__device__ __forceinline__ float dot4(const float4 a, float x, float y, float z) {
+    return fmaf(a.x, x, fmaf(a.y, y, fmaf(a.z, z, a.w)));
+}
+
+// EXACT: chord-length footprint (CB_backproject.cu:408-477).
+// RAYCAST: fast mode with direct-raycast weights (:512-646, preset 0).
+// BILIN: bilinear instead of nearest detector sampling.
+// ORD: 0 = C order (fastest axis z, slowest x), 1 = F order (fastest x).
+template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
+__global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
+    __shared__ ab_bpview sv[kChunk];
+    __shared__ ab_bpview_exact sx[EXACT ? kChunk : 1];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i0 = blockIdx.x * 32 + lane;
+    const int i1 = blockIdx.y * 8 + warp;
+    const int i2b = blockIdx.z * kXB;
+    constexpr int a0 = ORD == 0 ? 2 : 0, a1 = 1, a2 = ORD == 0 ? 0 : 2;
+    const bool in01 = i0 < P.n[a0] && i1 < P.n[a1];
+
+    // Voxel-centre coordinates relative to the volume centre, per axis.
+    const float vw = P.voxwid;
+    float base[3];
+    int idx[3];
+    idx[a0] = i0;
+    idx[a1] = i1;
+    idx[a2] = i2b;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) base[a] = ((float)idx[a] + 0.5f - 0.5f * (float)P.n[a]) * vw;
+
+    // Cylinder mask about world x = y = 0 (CB_backproject.cu:339-343); it
+    // depends on x and y only, so it may differ between the XB voxels when the
+    // slowest axis is x or y.
+    bool live[kXB];
+    bool any_live = false;
+#pragma unroll
+    for (int k = 0; k < kXB; ++k) {
+        float c[3] = {base[0], base[1], base[2]};
+        c[a2] += (float)k * vw;
+        bool ok = in01 && (i2b + k) < P.n[a2];
+        if (ok && P.mask) {
+            const float xw = c[0] + P.c0[0], yw = c[1] + P.c0[1];
+            ok = !(xw * xw + yw * yw > P.mask_r2);
+        }
+        live[k] = ok;
+        any_live |= ok;
+    }
+
+    float acc_x[kXB];
+#pragma unroll
+    for (int k = 0; k < kXB; ++k) acc_x[k] = 0.f;
+
+    const ab_d3 c0d{(double)P.c0[0], (double)P.c0[1], (double)P.c0[2]};
+    const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
+    for (int si = 0; si < P.ssx; ++si) {
+        float acc_y[kXB];
+#pragma unroll
+        for (int k = 0; k < kXB; ++k) acc_y[k] = 0.f;
+        for (int sj = 0; sj < P.ssy; ++sj) {
+            float acc_z[kXB];
+#pragma unroll
+            for (int k = 0; k < kXB; ++k) acc_z[k] = 0.f;
+            for (int sk = 0; sk < P.ssz; ++sk) {
+                const float sub[3] = {(-0.5f + offx * (0.5f + si)) * vw, (-0.5f + offy * (0.5f + sj)) * vw,
+                                      (-0.5f + offz * (0.5f + sk)) * vw};
+                float acc[kXB];
+#pragma unroll
+                for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
+                const float X0 = base[0] + sub[0], Y0 = base[1] + sub[1], Z0 = base[2] + sub[2];
+
+                for (uint32_t v0 = 0; v0 < P.n_views; v0 += kChunk) {
+                    const int cn = (int)min((uint32_t)kChunk, P.n_views - v0);
+                    __syncthreads();
+                    for (int t = threadIdx.x; t < cn; t += kThreads) {
+                        const aprict_proj_spec sp = P.specs[v0 + t];
+                        if (!ab_derive_bpview(sp, c0d, vw, sv[t]) && P.status)
+                            atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
+                        if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
+                    }
+                    __syncthreads();
+                    if (!any_live) continue;
+                    for (int t = 0; t < cn; ++t) {
+                        const int view = (int)v0 + t;
+                        const ab_bpview b = sv[t];
+                        const float Nu0 = dot4(b.nu, X0, Y0, Z0), Nv0 = dot4(b.nv, X0, Y0, Z0);
+                        const float D0 = dot4(b.den, X0, Y0, Z0);
+                        const float dNu = (a2 == 0 ? b.nu.x : (a2 == 1 ? b.nu.y : b.nu.z)) * vw;
+                        const float dNv = (a2 == 0 ? b.nv.x : (a2 == 1 ? b.nv.y : b.nv.z)) * vw;
+                        const float dD = (a2 == 0 ? b.den.x : (a2 == 1 ? b.den.y : b.den.z)) * vw;
+                        const bool needZ = RAYCAST ? (P.pL != 0 || P.pV != 0) : (P.pL != 0 || P.pV != 0);
+                        float Zb = 0.f, dZ = 0.f;
+                        if (needZ) {
+                            Zb = dot4(b.zl, X0, Y0, Z0);
+                            dZ = (a2 == 0 ? b.zl.x : (a2 == 1 ? b.zl.y : b.zl.z)) * vw;
+                        }
+#pragma unroll
+                        for (int k = 0; k < kXB; ++k) {
+                            if (!live[k]) continue;
+                            const float kf = (float)k;
+                            const float D = fmaf(kf, dD, D0);
+                            const float rD = 1.f / D;
+                            const float fu = fmaf(kf, dNu, Nu0) * rD;
+                            const float fv = fmaf(kf, dNv, Nv0) * rD;
+                            float s;
+                            if (EXACT) {
+                                // Footprint: bounding box of the 8 projected corners.
+                                const ab_bpview_exact e = sx[t];
+                                const float h = 0.5f * vw;
+                                const float hu[3] = {b.nu.x * h, b.nu.y * h, b.nu.z * h};
+                                const float hv[3] = {b.nv.x * h, b.nv.y * h, b.nv.z * h};
+                                const float hd[3] = {b.den.x * h, b.den.y * h, b.den.z * h};
+                                const float Nu = fmaf(kf, dNu, Nu0), Nv = fmaf(kf, dNv, Nv0);
+                                float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+#pragma unroll
+                                for (int c = 0; c < 8; ++c) {
+                                    const float sx_ = (c & 4) ? 1.f : -1.f, sy_ = (c & 2) ? 1.f : -1.f,
+                                                sz_ = (c & 1) ? 1.f : -1.f;
+                                    const float dd = D + sx_ * hd[0] + sy_ * hd[1] + sz_ * hd[2];
+                                    const float r = 1.f / dd;
+                                    const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * r;
+                                    const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * r;
+                                    umin = fminf(umin, uu);
+                                    umax = fmaxf(umax, uu);
+                                    vmin = fminf(vmin, vv);
+                                    vmax = fmaxf(vmax, vv);
+                                }
+                                const int ulo = max(0, (int)ceilf(umin - 1e-3f));
+                                const int uhi = min((int)P.nu - 1, (int)floorf(umax + 1e-3f));
+                                const int vlo = max(0, (int)ceilf(vmin - 1e-3f));
+                                const int vhi = min((int)P.nv - 1, (int)floorf(vmax + 1e-3f));
+                                // Ray origin relative to this voxel's centre.
+                                float cx[3] = {X0, Y0, Z0};
+                                cx[a2] += kf * vw;
+                                const float r0x = e.s.x - cx[0], r0y = e.s.y - cx[1], r0z = e.s.z - cx[2];
+                                const float *pb = P.projs + (int64_t)view * P.ps.view;
+                                s = 0.f;
+                                for (int iu = ulo; iu <= uhi; ++iu) {
+                                    const float dux = fmaf(e.u.x, (float)iu, e.d0.x);
+                                    const float duy = fmaf(e.u.y, (float)iu, e.d0.y);
+                                    const float duz = fmaf(e.u.z, (float)iu, e.d0.z);
+                                    for (int iv = vlo; iv <= vhi; ++iv) {
+                                        const float dx = fmaf(e.v.x, (float)iv, dux);
+                                        const float dy = fmaf(e.v.y, (float)iv, duy);
+                                        const float dz = fmaf(e.v.z, (float)iv, duz);
+                                        float a_lo = 0.f, a_hi = 3.0e38f;
+                                        bool miss = false;
+                                        if (dx != 0.f) {
+                                            const float inv = 1.f / dx;
+                                            const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
+                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                        } else {
+                                            miss |= fabsf(r0x) > h;
+                                        }
+                                        if (dy != 0.f) {
+                                            const float inv = 1.f / dy;
+                                            const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
+                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                        } else {
+                                            miss |= fabsf(r0y) > h;
+                                        }
+                                        if (dz != 0.f) {
+                                            const float inv = 1.f / dz;
+                                            const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
+                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                        } else {
+                                            miss |= fabsf(r0z) > h;
+                                        }
+                                        if (miss || !(a_hi > a_lo)) continue;
+                                        const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
+                                        const float pv =
+                                            P.all_ones ? 1.f
+                                                       : __ldg(pb + (int64_t)iu * P.ps.u + (int64_t)iv * P.ps.v);
+                                        s = fmaf(pv, chord, s);
+                                    }
+                                }
+                                if (needZ) {
+                                    const float Z = fmaf(kf, dZ, Zb);
+                                    if (P.pL != 0) s *= ab_powint(Z * b.invL, P.pL);
+                                    if (P.pV != 0) s *= ab_powint(Z / P.val, P.pV);
+                                }
+                            } else {
+                                float w;
+                                if (RAYCAST) {
+                                    w = 1.f;
+                                    if (needZ) {
+                                        const float Z = fmaf(kf, dZ, Zb);
+                                        if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
+                                        if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
+                                    }
+                                } else {
+                                    // (|p - s| / |x - s|)^2 * voxwid^3 / pixel area (:648-690)
+                                    w = b.kfast * rD * rD;
+                                    if (needZ) {
+                                        const float Z = fmaf(kf, dZ, Zb);
+                                        if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
+                                        if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
+                                    }
+                                }
+                                float pv = 0.f;
+                                if (w != 0.f) {
+                                    if (BILIN) {
+                                        pv = fetch_bilinear(P, view, fu, fv);
+                                    } else {
+                                        float xw[3] = {X0 + P.c0[0], Y0 + P.c0[1], Z0 + P.c0[2]};
+                                        xw[a2] += kf * vw;
+                                        pv = fetch_nearest(P, view, fu, fv, xw);
+                                    }
+                                }
+                                s = pv * w;
+                            }
+                            if (P.sep > 0.f && s != 0.f) {
+                                s *= ab_edge_taper(fu - (b.halfu - 0.5f), fv - (b.halfv - 0.5f), b.halfu, b.halfv,
+                                                   P.sep);
+                            }
+                            acc[k] += s;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kXB; ++k) acc_z[k] += acc[k];
+            }
+#pragma unroll
+            for (int k = 0; k < kXB; ++k) acc_y[k] += acc_z[k] / (float)P.ssz;
+        }
+#pragma unroll
+        for (int k = 0; k < kXB; ++k) acc_x[k] += acc_y[k] / (float)P.ssy;
+    }
+
+#pragma unroll
+    for (int k = 0; k < kXB; ++k) {
+        if (!live[k]) continue;
+        const float value = acc_x[k] / (float)P.ssx;
+        if (value == 0.f) continue;  // the reference skips the write (:1010)
+        int id[3];
+        id[a0] = i0;
+        id[a1] = i1;
+        id[a2] = i2b + k;
+        const int64_t o = (int64_t)id[0] * P.vs[0] + (int64_t)id[1] * P.vs[1] + (int64_t)id[2] * P.vs[2];
+        const float m = P.mult ? P.mult[o] : 1.f;
+        P.vol[o] = value * m + P.vol[o];
+    }
+}
+
+template <int ORD>
+void launch_bp(const BPParams &P, const aprict_backproject_config *cfg, bool lin, dim3 grid, cudaStream_t st) {
+    if (cfg->exact) {
+        k_backproject<ORD, true, false, false><<<grid, kThreads, 0, st>>>(P);
+    } else if (cfg->approx_mode_direct_raycast) {
+        if (lin)
+            k_backproject<ORD, false, true, true><<<grid, kThreads, 0, st>>>(P);
+        else
+            k_backproject<ORD, false, true, false><<<grid, kThreads, 0, st>>>(P);
+    } else {
+        if (lin)
+            k_backproject<ORD, false, false, true><<<grid, kThreads, 0, st>>>(P);
+        else
+            k_backproject<ORD, false, false, false><<<grid, kThreads, 0, st>>>(P);
+    }
+}
+
+}  // namespace
+
+extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                       const float *projs_dev, const aprict_vol_desc *vd, float *vol_dev,
+                                       const float *multiplier_dev, const aprict_backproject_config *cfg,
+                                       uint32_t *status_dev, aprict_stream_t stream) {
+    int rc;
+    if ((rc = ab_check_projs(pd, projs_dev, "projections")) != APRICT_OK) return rc;
+    if ((rc = ab_check_vol(vd, vol_dev, "volume")) != APRICT_OK) return rc;
+    if (cfg == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null backproject config");
+    if (cfg->apply_summand_multiplier != (multiplier_dev != nullptr ? 1u : 0u))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
+                       "apply_summand_multiplier must be set if and only if a multiplier is given");
+    if (cfg->weighting_preset != 0)
+        return ab_fail(APRICT_ERR_UNSUPPORTED, "backprojection weighting preset %u is not implemented",
+                       cfg->weighting_preset);
+    if (cfg->ssx == 0 || cfg->ssy == 0 || cfg->ssz == 0 || cfg->ssx > 16 || cfg->ssy > 16 || cfg->ssz > 16)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ssx/ssy/ssz must be in [1, 16]");
+    if (cfg->Z_on_val_factor_power != 0 && !(cfg->Z_on_val_factor_val != 0.f))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "Z_on_val_factor_val must be nonzero");
+    if (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) return APRICT_OK;
+    if (specs_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null view specs");
+    if (multiplier_dev && (reinterpret_cast<uintptr_t>(multiplier_dev) & 3u))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "multiplier pointer not 4-byte aligned");
+
+    BPParams P{};
+    P.specs = specs_dev;
+    P.n_views = pd->n_views;
+    P.nu = pd->nu;
+    P.nv = pd->nv;
+    P.ps = ab_pstrides{pd->stride_view, pd->stride_u, pd->stride_v};
+    P.projs = projs_dev;
+    P.vol = vol_dev;
+    P.mult = multiplier_dev;
+    P.n[0] = (int)vd->nx;
+    P.n[1] = (int)vd->ny;
+    P.n[2] = (int)vd->nz;
+    if (vd->order == 0) {
+        P.vs[0] = (int64_t)vd->ny * vd->nz;
+        P.vs[1] = vd->nz;
+        P.vs[2] = 1;
+    } else {
+        P.vs[0] = 1;
+        P.vs[1] = vd->nx;
+        P.vs[2] = (int64_t)vd->nx * vd->ny;
+    }
+    P.voxwid = vd->voxwid;
+    P.c0[0] = vd->corner.x + 0.5f * vd->voxwid * (float)vd->nx;
+    P.c0[1] = vd->corner.y + 0.5f * vd->voxwid * (float)vd->ny;
+    P.c0[2] = vd->corner.z + 0.5f * vd->voxwid * (float)vd->nz;
+    P.mask = cfg->mask_to_cylinder ? 1 : 0;
+    P.mask_r2 = cfg->mask_to_cyl_rad * cfg->mask_to_cyl_rad;
+    P.all_ones = cfg->backproject_all_1s ? 1 : 0;
+    P.sep = cfg->soften_edge_proportion;
+    P.pL = cfg->Z_on_L_factor_power;
+    P.pV = cfg->Z_on_val_factor_power;
+    P.val = cfg->Z_on_val_factor_val;
+    P.ssx = (int)cfg->ssx;
+    P.ssy = (int)cfg->ssy;
+    P.ssz = (int)cfg->ssz;
+    P.status = status_dev;
+
+    const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
+    dim3 grid((unsigned)((n0 + 31) / 32), (unsigned)((n1 + 7) / 8), (unsigned)((n2 + kXB - 1) / kXB));
+    if (grid.y > 65535u || grid.z > 65535u) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const bool lin = cfg->approx_mode_linear_interpolate != 0;
+    if (vd->order == 0)
+        launch_bp<0>(P, cfg, lin, grid, st);
+    else
+        launch_bp<1>(P, cfg, lin, grid, st);
+    return ab_cuda_check(cudaGetLastError(), "backproject launch");
+}

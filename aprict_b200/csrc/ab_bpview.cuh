@@ -1,0 +1,122 @@
+// ab_bpview.cuh -- per-view coefficients for voxel-driven backprojection.
+//
+// The reference re-derives, for every voxel and view, the detector
+// coordinates of a point with get_projected_detector_coords
+// (src/aprict/data/cusrc/geometry.h:24-56): a cross product, two norms and
+// three divisions in FP32. Here each view is reduced once (in FP64, per CTA,
+// into shared memory) to three linear forms of the voxel position x, taken
+// relative to the volume centre c0:
+//
+//   den(x) = (x - s).n                      n = u x v (detector normal)
+//   Nu(x)  = A_u.(x - c0) + B_u             u index = Nu(x) / den(x)
+//   Nv(x)  = A_v.(x - c0) + B_v             v index = Nv(x) / den(x)
+//
+// which is the same mapping: with Dn = (P - s).n and lambda = Dn / den(x),
+// q = s + (x - s) lambda - P, cu = u.q/|u|^2, so
+//   cu * den = [Dn u - (u.(P - s)) n].(x - s) / |u|^2,
+// and the pixel index is cu + (nu-1)/2. Shifting the origin to c0 keeps the
+// FP32 terms of the dot products small.
+#pragma once
+
+#include "ab_common.cuh"
+
+struct ab_bpview {
+    float4 nu;   // A_u.xyz, B_u
+    float4 nv;   // A_v.xyz, B_v
+    float4 den;  // n.xyz,  (c0 - s).n
+    float4 zl;   // Lhat.xyz, (c0 - s).Lhat  ->  Z(x) = distance along L = P - s
+    float kfast; // voxwid^3 Dn^2 / (|u||v|): fast-mode weight is kfast / den^2
+    float invL;  // 1 / |L|
+    float halfu; // nu / 2
+    float halfv; // nv / 2
+};
+
+// Exact-mode extras: ray origin and per-pixel direction in world units,
+// relative to the volume centre.
+struct ab_bpview_exact {
+    float4 s;   // s - c0 (xyz), unused
+    float4 d0;  // direction to the detector centre pixel origin: P - s - u(nu-1)/2 - v(nv-1)/2
+    float4 u;   // det_u
+    float4 v;   // det_v
+};
+
+AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, ab_bpview &o) {
+    const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
+    const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);
+    const ab_d3 n = ab_cross(U, V);
+    const double uu = ab_dot(U, U), vv = ab_dot(V, V);
+    const ab_d3 Ps = P - s;
+    const double Dn = ab_dot(Ps, n);
+    const ab_d3 c0s = c0 - s;
+    const double Lnorm = sqrt(ab_dot(Ps, Ps));
+    bool ok = uu > 0.0 && vv > 0.0 && Dn != 0.0 && Lnorm > 0.0 && ab_finite3(s) && ab_finite3(P) &&
+              ab_finite3(U) && ab_finite3(V);
+    if (!ok) {
+        o = ab_bpview{};
+        return false;
+    }
+    const double hu = ((double)sp.nu - 1.0) * 0.5, hv = ((double)sp.nv - 1.0) * 0.5;
+    // A_u = (Dn U - (U.(P-s)) n) / |U|^2 + hu n ;  B_u = A_u.(c0 - s)
+    const ab_d3 Au = (U * Dn - n * ab_dot(U, Ps)) * (1.0 / uu) + n * hu;
+    const ab_d3 Av = (V * Dn - n * ab_dot(V, Ps)) * (1.0 / vv) + n * hv;
+    const ab_d3 Lh = Ps * (1.0 / Lnorm);
+    o.nu = make_float4((float)Au.x, (float)Au.y, (float)Au.z, (float)ab_dot(Au, c0s));
+    o.nv = make_float4((float)Av.x, (float)Av.y, (float)Av.z, (float)ab_dot(Av, c0s));
+    o.den = make_float4((float)n.x, (float)n.y, (float)n.z, (float)ab_dot(n, c0s));
+    o.zl = make_float4((float)Lh.x, (float)Lh.y, (float)Lh.z, (float)ab_dot(Lh, c0s));
+    const double vw = (double)voxwid;
+    o.kfast = (float)(vw * vw * vw * Dn * Dn / (sqrt(uu) * sqrt(vv)));
+    o.invL = (float)(1.0 / Lnorm);
+    o.halfu = (float)sp.nu * 0.5f;
+    o.halfv = (float)sp.nv * 0.5f;
+    return true;
+}
+
+AB_HD void ab_derive_bpview_exact(const aprict_proj_spec &sp, ab_d3 c0, ab_bpview_exact &o) {
+    const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
+    const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);
+    const double hu = ((double)sp.nu - 1.0) * 0.5, hv = ((double)sp.nv - 1.0) * 0.5;
+    const ab_d3 sr = s - c0;
+    const ab_d3 d0 = P - s - U * hu - V * hv;
+    o.s = make_float4((float)sr.x, (float)sr.y, (float)sr.z, 0.f);
+    o.d0 = make_float4((float)d0.x, (float)d0.y, (float)d0.z, 0.f);
+    o.u = make_float4((float)U.x, (float)U.y, (float)U.z, 0.f);
+    o.v = make_float4((float)V.x, (float)V.y, (float)V.z, 0.f);
+}
+
+// FP64 detector index coordinates of world point x (reference formula,
+// geometry.h:39-51, in double), used to settle nearest-pixel choices that
+// the FP32 path cannot resolve.
+AB_HD void ab_project_point_d(const aprict_proj_spec &sp, ab_d3 x, double &fu, double &fv) {
+    const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
+    const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);
+    const ab_d3 n = ab_cross(U, V);
+    const double lam = ab_dot(P - s, n) / ab_dot(x - s, n);
+    const ab_d3 q = s + (x - s) * lam - P;
+    fu = ab_dot(U, q) / ab_dot(U, U) + ((double)sp.nu - 1.0) * 0.5;
+    fv = ab_dot(V, q) / ab_dot(V, V) + ((double)sp.nv - 1.0) * 0.5;
+}
+
+// Integer power as in the reference's powint (CB_backproject.cu:21-35).
+AB_HD float ab_powint(float b, int e) {
+    float a = 1.f;
+    if (e < 0) {
+        for (int k = 0; k < -e; ++k) a /= b;
+    } else {
+        for (int k = 0; k < e; ++k) a *= b;
+    }
+    return a;
+}
+
+// Detector-edge cosine taper (CB_backproject.cu:694-713); cu, cv are
+// coordinates relative to the detector centre in pixels.
+AB_HD float ab_edge_taper(float cu, float cv, float halfu, float halfv, float sep) {
+    float ud = fabsf(cu) / halfu;
+    float vd = fabsf(cv) / halfv;
+    ud = fmaxf(0.f, fminf(1.f, (1.f - ud) / sep));
+    vd = fmaxf(0.f, fminf(1.f, (1.f - vd) / sep));
+    // (1 + cos(pi (1 - x))) / 2 == (1 - cos(pi x)) / 2
+    ud = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - ud))) * 0.5f));
+    vd = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - vd))) * 0.5f));
+    return ud * vd;
+}

@@ -1,0 +1,215 @@
+// ab_common.cuh -- shared device helpers for the aprict_b200 kernels.
+//
+// Geometry conventions follow the reference (murdock-grewar/aprict 0.1.5):
+//   * voxel (i,j,k) of an (X,Y,Z) volume occupies
+//     [corner + voxwid*(i,j,k), corner + voxwid*(i+1,j+1,k+1)) in world units
+//     (src/aprict/volume/volume.py:133-145, flatpanel.py:1025-1041);
+//   * pixel (iu,iv) centre = det_pos + det_u*(iu-(nu-1)/2) + det_v*(iv-(nv-1)/2)
+//     (src/aprict/data/cusrc/CB_project_texture_chunked.cu:308-324).
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#include "aprict_b200.h"
+
+#if defined(__CUDACC__)
+#define AB_HD __host__ __device__ __forceinline__
+#define AB_DEV __device__ __forceinline__
+#else
+#define AB_HD inline
+#define AB_DEV inline
+#endif
+
+// ---------------------------------------------------------------------------
+// Small double-precision vector helpers (ray setup is done in FP64).
+struct ab_d3 {
+    double x, y, z;
+};
+AB_HD ab_d3 ab_d3_of(aprict_fvec3 v) { return ab_d3{(double)v.x, (double)v.y, (double)v.z}; }
+AB_HD ab_d3 operator+(ab_d3 a, ab_d3 b) { return ab_d3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+AB_HD ab_d3 operator-(ab_d3 a, ab_d3 b) { return ab_d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+AB_HD ab_d3 operator*(ab_d3 a, double s) { return ab_d3{a.x * s, a.y * s, a.z * s}; }
+AB_HD double ab_dot(ab_d3 a, ab_d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+AB_HD ab_d3 ab_cross(ab_d3 a, ab_d3 b) {
+    return ab_d3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+AB_HD bool ab_finite3(ab_d3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+// Volume geometry as the traversal sees it: voxel units, corner at the origin.
+template <typename Off>
+struct ab_grid {
+    int n[3];         // X, Y, Z
+    Off stride[3];    // element strides of x, y, z
+    double corner[3]; // world
+    double inv_voxwid;
+    float voxwid;
+};
+
+template <typename Off>
+AB_HD ab_grid<Off> ab_make_grid(const aprict_vol_desc &v) {
+    ab_grid<Off> g;
+    g.n[0] = (int)v.nx;
+    g.n[1] = (int)v.ny;
+    g.n[2] = (int)v.nz;
+    if (v.order == 0) {  // C order: z fastest
+        g.stride[0] = (Off)v.ny * (Off)v.nz;
+        g.stride[1] = (Off)v.nz;
+        g.stride[2] = 1;
+    } else {  // F order: x fastest
+        g.stride[0] = 1;
+        g.stride[1] = (Off)v.nx;
+        g.stride[2] = (Off)v.nx * (Off)v.ny;
+    }
+    g.corner[0] = v.corner.x;
+    g.corner[1] = v.corner.y;
+    g.corner[2] = v.corner.z;
+    g.voxwid = v.voxwid;
+    g.inv_voxwid = 1.0 / (double)v.voxwid;
+    return g;
+}
+
+// World point -> voxel units relative to the grid corner.
+template <typename Off>
+AB_HD ab_d3 ab_to_grid(const ab_grid<Off> &g, ab_d3 p) {
+    return ab_d3{(p.x - g.corner[0]) * g.inv_voxwid, (p.y - g.corner[1]) * g.inv_voxwid,
+                 (p.z - g.corner[2]) * g.inv_voxwid};
+}
+
+// ---------------------------------------------------------------------------
+// Siddon traversal of the segment o -> e (voxel units, grid corner at 0).
+//
+// Computes the same quantity as exact_line_integral_unitvoxwid
+// (CB_project_texture_chunked.cu:111-272): the exact intersection length of
+// the segment with every voxel it crosses. The arithmetic differs on purpose:
+//   * entry/exit parameters, the entry voxel and every per-axis crossing
+//     origin are computed in FP64;
+//   * crossings are stepped in FP32 as tau_a(k) = t0_a + k*dt_a (one fma per
+//     step, relative to the entry point), so positions never drift -- the
+//     reference adds steps*d to a running position and accumulates error;
+//   * the visitor receives (segment length in voxel units, element offset).
+// Tie rules mirror the reference: a coordinate exactly on a voxel boundary
+// belongs to the voxel the ray moves into; with zero direction along an axis
+// the voxel is ceil(c)-1 (reference :189-203, :244-246), so a ray lying in the
+// plane c == 0 misses and one in c == n hits the last layer.
+//
+// Returns false (visiting nothing) when the segment misses the grid or its
+// input is not finite; *bad is set for non-finite input.
+template <typename Off, class Visit>
+AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visit &visit, bool *bad) {
+    if (!ab_finite3(o) || !ab_finite3(e)) {
+        *bad = true;
+        return false;
+    }
+    const double od[3] = {o.x, o.y, o.z};
+    const double dd[3] = {e.x - o.x, e.y - o.y, e.z - o.z};
+    double a_in = 0.0, a_out = 1.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (dd[a] == 0.0) {
+            if (!(od[a] > 0.0 && od[a] <= (double)n[a])) return false;
+        } else {
+            const double inv = 1.0 / dd[a];
+            const double t0 = (0.0 - od[a]) * inv;
+            const double t1 = ((double)n[a] - od[a]) * inv;
+            a_in = fmax(a_in, fmin(t0, t1));
+            a_out = fmin(a_out, fmax(t0, t1));
+        }
+    }
+    if (!(a_in < a_out)) return false;
+    const double len = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+
+    int idx[3], lim[3], stp[3];
+    float t0f[3], dtf[3];
+    Off off = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double p = od[a] + a_in * dd[a];
+        int i;
+        if (dd[a] > 0.0) {
+            i = (int)floor(p);
+        } else {
+            i = (int)ceil(p) - 1;
+        }
+        i = i < 0 ? 0 : (i >= n[a] ? n[a] - 1 : i);
+        idx[a] = i;
+        off += (Off)i * stride[a];
+        if (dd[a] == 0.0) {
+            stp[a] = 0;
+            lim[a] = -2;  // never reached
+            t0f[a] = INFINITY;
+            dtf[a] = 0.f;
+        } else {
+            const bool pos = dd[a] > 0.0;
+            stp[a] = pos ? 1 : -1;
+            lim[a] = pos ? n[a] : -1;
+            const double b = pos ? (double)(i + 1) : (double)i;
+            const double ab = (b - od[a]) / dd[a];
+            t0f[a] = (float)((ab - a_in) * len);
+            dtf[a] = (float)(len / fabs(dd[a]));
+        }
+    }
+    const float tend = (float)((a_out - a_in) * len);
+    // Scalars (not arrays) in the loop keep everything in registers.
+    int ix = idx[0], iy = idx[1], iz = idx[2];
+    const int lx = lim[0], ly = lim[1], lz = lim[2];
+    const Off ox = stp[0] > 0 ? stride[0] : (Off)0 - stride[0];
+    const Off oy = stp[1] > 0 ? stride[1] : (Off)0 - stride[1];
+    const Off oz = stp[2] > 0 ? stride[2] : (Off)0 - stride[2];
+    const int sx = stp[0], sy = stp[1], sz = stp[2];
+    const float t0x = t0f[0], t0y = t0f[1], t0z = t0f[2];
+    const float dtx = dtf[0], dty = dtf[1], dtz = dtf[2];
+    float kx = 0.f, ky = 0.f, kz = 0.f;
+    float tx = t0x, ty = t0y, tz = t0z;
+    float t = 0.f;
+    for (;;) {
+        const float tm = fminf(tx, fminf(ty, tz));
+        const float te = fminf(tm, tend);
+        visit(te - t, off);
+        if (tm >= tend) break;
+        t = tm;
+        if (tx == tm) {
+            ix += sx;
+            if (ix == lx) break;
+            off += ox;
+            kx += 1.f;
+            tx = fmaf(kx, dtx, t0x);
+        } else if (ty == tm) {
+            iy += sy;
+            if (iy == ly) break;
+            off += oy;
+            ky += 1.f;
+            ty = fmaf(ky, dty, t0y);
+        } else {
+            iz += sz;
+            if (iz == lz) break;
+            off += oz;
+            kz += 1.f;
+            tz = fmaf(kz, dtz, t0z);
+        }
+    }
+    return true;
+}
+
+// Kahan-compensated FP32 accumulator.
+struct ab_kahan {
+    float s, c;
+    AB_HD void add(float v) {
+        const float y = v - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// Pixel centre (fractional index) in world units, FP64 from the FP32 spec.
+AB_HD ab_d3 ab_pixel_pos(const aprict_proj_spec &sp, double fu, double fv) {
+    const double xnum = fu - ((double)sp.nu - 1.0) * 0.5;
+    const double ynum = fv - ((double)sp.nv - 1.0) * 0.5;
+    return ab_d3_of(sp.det_pos) + ab_d3_of(sp.det_u) * xnum + ab_d3_of(sp.det_v) * ynum;
+}
+
+// Element offsets into a projection stack.
+struct ab_pstrides {
+    int64_t view, u, v;
+};

@@ -1,0 +1,219 @@
+// ab_siddon.cu -- Siddon forward projector and its ray-driven matched adjoint.
+//
+// Forward: replaces project_CB_texture_chunked<float,float>
+// (src/aprict/data/cusrc/CB_project_texture_chunked.cu:327-412). One thread
+// per (view, pixel); ssu x ssv sub-rays averaged as in :381-407; result
+// scaled by multiply_before_adding (:394) and accumulated (:411).
+//
+// B200 layout: a CTA covers a 2-D detector tile of one view and each warp a
+// 4 (u) x 8 (v) pixel patch, so the rays of a warp are spatially coherent and
+// their voxel gathers hit the same L1 lines; 8 consecutive v per row make the
+// output access one 32-byte sector. CTAs are ordered view-major so the CTAs
+// resident at one time cover 1-2 views and share the volume working set in L2.
+#include <cuda_runtime.h>
+
+#include "ab_common.cuh"
+#include "ab_host.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct TileMap {
+    int tile_u, tile_v;  // tile extents in pixels
+    int ntu, ntv;        // number of tiles along u, v
+};
+
+// Tile shapes: tv == 1 -> one detector row per tile (used when nv < 8);
+// otherwise warps are 4 (u) x 8 (v) patches.
+TileMap make_tiles(uint32_t nu, uint32_t nv) {
+    TileMap t;
+    t.tile_v = nv >= 16 ? 16 : (nv >= 8 ? 8 : 1);
+    t.tile_u = kThreads / t.tile_v;
+    t.ntu = (int)((nu + t.tile_u - 1) / t.tile_u);
+    t.ntv = (int)((nv + t.tile_v - 1) / t.tile_v);
+    return t;
+}
+
+__device__ __forceinline__ void tile_pixel(const TileMap &tm, int tile, int &iu, int &iv) {
+    const int tu = tile % tm.ntu;
+    const int tv = tile / tm.ntu;
+    const int t = threadIdx.x;
+    if (tm.tile_v == 1) {
+        iu = tu * tm.tile_u + t;
+        iv = tv;
+    } else {
+        const int lane = t & 31, warp = t >> 5;
+        const int wv_per = tm.tile_v / 8;  // warps along v in the tile
+        const int wu = warp / wv_per, wv = warp % wv_per;
+        iu = tu * tm.tile_u + wu * 4 + (lane >> 3);
+        iv = tv * tm.tile_v + wv * 8 + (lane & 7);
+    }
+}
+
+template <typename Off>
+struct GatherVisit {
+    const float *__restrict__ vol;
+    ab_kahan acc;
+    __device__ __forceinline__ void operator()(float seg, Off off) { acc.add(seg * __ldg(vol + off)); }
+};
+
+template <typename Off>
+struct ScatterVisit {
+    float *__restrict__ vol;
+    float w;
+    __device__ __forceinline__ void operator()(float seg, Off off) {
+        if (seg > 0.f) atomicAdd(vol + off, seg * w);
+    }
+};
+
+
+template <typename Off>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_project_siddon(const aprict_proj_spec *__restrict__ specs, uint32_t n_views, uint32_t nu, uint32_t nv,
+                     ab_pstrides ps, float *__restrict__ out, const float *base, ab_grid<Off> g, const float *vol,
+                     float svf, float mba, int ssu, int ssv, TileMap tm, uint32_t view0, uint32_t *status) {
+    const uint32_t view = view0 + blockIdx.y;
+    if (view >= n_views) return;
+    int iu, iv;
+    tile_pixel(tm, blockIdx.x, iu, iv);
+    if (iu >= (int)nu || iv >= (int)nv) return;
+    const aprict_proj_spec sp = specs[view];
+    const ab_d3 src = ab_to_grid(g, ab_d3_of(sp.source_pos) * (double)svf);
+
+    bool bad = false;
+    float tot = 0.f;
+    const double inv_su = 1.0 / (double)ssu, inv_sv = 1.0 / (double)ssv;
+    for (int ku = 0; ku < ssu; ++ku) {
+        float accu = 0.f;
+        for (int kv = 0; kv < ssv; ++kv) {
+            const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
+            const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
+            const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)svf);
+            GatherVisit<Off> vis{vol, {0.f, 0.f}};
+            ab_siddon<Off>(src, dst, g.n, g.stride, vis, &bad);
+            accu += (vis.acc.s * g.voxwid) * mba;
+        }
+        if (ssv > 1) accu /= (float)ssv;
+        tot += accu;
+    }
+    if (ssu > 1) tot /= (float)ssu;
+    if (bad && status) atomicOr(status, APRICT_STATUS_NONFINITE);
+    const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
+    if (base) {
+        out[o] = base[o] + tot;
+    } else {
+        atomicAdd(out + o, tot);
+    }
+}
+
+template <typename Off>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_backproject_scatter(const aprict_proj_spec *__restrict__ specs, uint32_t n_views, uint32_t nu, uint32_t nv,
+                          ab_pstrides ps, const float *__restrict__ projs, ab_grid<Off> g, float *vol, float svf,
+                          float mba, int ssu, int ssv, TileMap tm, uint32_t view0, uint32_t *status) {
+    const uint32_t view = view0 + blockIdx.y;
+    if (view >= n_views) return;
+    int iu, iv;
+    tile_pixel(tm, blockIdx.x, iu, iv);
+    if (iu >= (int)nu || iv >= (int)nv) return;
+    const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
+    const float p = projs[o];
+    if (p == 0.f) return;
+    const aprict_proj_spec sp = specs[view];
+    const ab_d3 src = ab_to_grid(g, ab_d3_of(sp.source_pos) * (double)svf);
+    // Transpose of: out = (1/ssu) sum_ku (1/ssv) sum_kv mba * voxwid * sum_seg seg*mu
+    const float w = p * mba * g.voxwid / (float)(ssu * ssv);
+    bool bad = false;
+    const double inv_su = 1.0 / (double)ssu, inv_sv = 1.0 / (double)ssv;
+    for (int ku = 0; ku < ssu; ++ku) {
+        for (int kv = 0; kv < ssv; ++kv) {
+            const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
+            const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
+            const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)svf);
+            ScatterVisit<Off> vis{vol, w};
+            ab_siddon<Off>(src, dst, g.n, g.stride, vis, &bad);
+        }
+    }
+    if (bad && status) atomicOr(status, APRICT_STATUS_NONFINITE);
+}
+
+int check_common(const aprict_proj_spec *specs, const aprict_proj_desc *pd, const void *pptr,
+                 const aprict_vol_desc *vd, const void *vptr, const aprict_project_config *cfg) {
+    int rc;
+    if ((rc = ab_check_projs(pd, pptr, "projections")) != APRICT_OK) return rc;
+    if ((rc = ab_check_vol(vd, vptr, "volume")) != APRICT_OK) return rc;
+    if (cfg == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null project config");
+    if (cfg->ssu == 0 || cfg->ssv == 0 || cfg->ssu > 64 || cfg->ssv > 64)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ssu/ssv must be in [1, 64]");
+    if (!isfinite(cfg->shrink_volume_factor) || !isfinite(cfg->multiply_before_adding))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "non-finite project config");
+    if (pd->n_views && specs == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null view specs");
+    return APRICT_OK;
+}
+
+bool small_volume(const aprict_vol_desc *vd) {
+    return (uint64_t)vd->nx * vd->ny * vd->nz < (1ull << 31);
+}
+
+}  // namespace
+
+extern "C" int aprict_b200_project_siddon(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                          float *projs_dev, const float *base_dev, const aprict_vol_desc *vd,
+                                          const float *vol_dev, const aprict_project_config *cfg,
+                                          uint32_t *status_dev, aprict_stream_t stream) {
+    int rc = check_common(specs_dev, pd, projs_dev, vd, vol_dev, cfg);
+    if (rc != APRICT_OK) return rc;
+    if (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) return APRICT_OK;
+    const TileMap tm = make_tiles(pd->nu, pd->nv);
+    const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    for (uint32_t v0 = 0; v0 < pd->n_views; v0 += 65535u) {
+        const uint32_t nvw = pd->n_views - v0 < 65535u ? pd->n_views - v0 : 65535u;
+        dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
+        if (small_volume(vd)) {
+            k_project_siddon<int32_t><<<grid, kThreads, 0, st>>>(
+                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int32_t>(*vd),
+                vol_dev, cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm,
+                v0, status_dev);
+        } else {
+            k_project_siddon<int64_t><<<grid, kThreads, 0, st>>>(
+                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int64_t>(*vd),
+                vol_dev, cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm,
+                v0, status_dev);
+        }
+        rc = ab_cuda_check(cudaGetLastError(), "project_siddon launch");
+        if (rc != APRICT_OK) return rc;
+    }
+    return APRICT_OK;
+}
+
+extern "C" int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                               const float *projs_dev, const aprict_vol_desc *vd, float *vol_dev,
+                                               const aprict_project_config *cfg, uint32_t *status_dev,
+                                               aprict_stream_t stream) {
+    int rc = check_common(specs_dev, pd, projs_dev, vd, vol_dev, cfg);
+    if (rc != APRICT_OK) return rc;
+    if (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) return APRICT_OK;
+    const TileMap tm = make_tiles(pd->nu, pd->nv);
+    const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    for (uint32_t v0 = 0; v0 < pd->n_views; v0 += 65535u) {
+        const uint32_t nvw = pd->n_views - v0 < 65535u ? pd->n_views - v0 : 65535u;
+        dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
+        if (small_volume(vd)) {
+            k_backproject_scatter<int32_t><<<grid, kThreads, 0, st>>>(
+                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int32_t>(*vd), vol_dev,
+                cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, v0,
+                status_dev);
+        } else {
+            k_backproject_scatter<int64_t><<<grid, kThreads, 0, st>>>(
+                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int64_t>(*vd), vol_dev,
+                cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, v0,
+                status_dev);
+        }
+        rc = ab_cuda_check(cudaGetLastError(), "backproject_scatter launch");
+        if (rc != APRICT_OK) return rc;
+    }
+    return APRICT_OK;
+}

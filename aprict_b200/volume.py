@@ -1,0 +1,330 @@
+"""Voxel volumes (``Volume``) and analytic FORBILD phantoms (``FBVolume``).
+
+Mirrors ``aprict.volume`` (src/aprict/volume/volume.py:51-495). The reference
+stores a ``Volume`` in a CUDA array behind a surface object; users never touch
+the texture (src/aprict/volume/volume.py:18-20), so here the storage is a
+linear float32 device buffer (a torch tensor with C- or F-order strides) that
+the kernels index directly. Voxel centres follow the reference convention:
+``pos_c + voxwid * (i - (n-1)/2)`` (volume.py:133-145).
+"""
+
+from __future__ import annotations
+
+import pathlib
+import typing
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_SUPPORTED_DTYPES = (np.dtype(np.float32),)
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        msg = "aprict_b200 needs a CUDA device (B200, sm_100a); none is available"
+        raise RuntimeError(msg)
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _empty(shape: tuple[int, int, int], order: str) -> torch.Tensor:
+    X, Y, Z = shape
+    strides = (Y * Z, Z, 1) if order == "C" else (1, X, X * Y)
+    return torch.empty_strided(shape, strides, dtype=torch.float32, device=_device())
+
+
+class Volume:
+    """A rectangular prism of voxels, stored on the GPU."""
+
+    _shape: tuple[int, int, int]
+    _dtype: np.dtype
+    _order: typing.Literal["C", "F"]
+    _data: torch.Tensor
+    _pos_c: np.ndarray
+    _voxwid: float
+
+    def __init__(
+        self,
+        arr: np.ndarray | torch.Tensor,
+        *,
+        voxwid: float,
+        pos_c: np.ndarray | tuple[float, float, float] = (0.0, 0.0, 0.0),
+        initialize_texture: bool = True,
+        order: typing.Literal["C", "F"] = "C",
+    ) -> None:
+        if order not in ("C", "F"):
+            msg = f"order must be 'C' or 'F', not {order!r}"
+            raise ValueError(msg)
+        if tuple(arr.shape).__len__() != 3:
+            msg = "Volume arrays must be 3-dimensional (X, Y, Z)."
+            raise ValueError(msg)
+        dt = np.dtype(str(arr.dtype).replace("torch.", ""))
+        if dt not in _SUPPORTED_DTYPES:
+            msg = f"Volume dtype {dt} is not supported (float32 only)."
+            raise NotImplementedError(msg)
+        self._dtype = dt
+        self._shape = tuple(int(s) for s in arr.shape)  # type: ignore[assignment]
+        self._order = order
+        self._voxwid = float(voxwid)
+        self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
+        if initialize_texture:
+            self._data = _empty(self._shape, order)
+            self.copy_from(arr)
+
+    # ------------------------------------------------------------------ props
+    @property
+    def voxwid(self) -> float:
+        """The width of each voxel."""
+        return self._voxwid
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        """The shape (X, Y, Z) of the volume."""
+        return self._shape
+
+    @property
+    def dtype(self) -> np.dtype:
+        """The dtype of the volume."""
+        return self._dtype
+
+    @property
+    def order(self) -> str:
+        """Memory order of the device buffer: 'C' (z fastest) or 'F' (x fastest)."""
+        return self._order
+
+    @property
+    def data(self) -> torch.Tensor:
+        """The device tensor (shape (X,Y,Z), strides per ``order``); shared, not copied."""
+        return self._data
+
+    @property
+    def pos_c(self) -> np.ndarray:
+        """Position of the centre of the volume."""
+        return self._pos_c.copy()
+
+    @property
+    def corner(self) -> np.ndarray:
+        """World position of the outer corner of voxel (0,0,0) (flatpanel.py:1030-1036)."""
+        return self._pos_c - np.float32(self._voxwid) * np.array(self._shape, dtype=np.float32) / 2
+
+    @property
+    def norm(self) -> float:
+        """The l2 norm of the volume (double accumulation)."""
+        return float(np.sqrt(self.inner_product(self)))
+
+    @property
+    def xs_ys_zs(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Voxel-centre coordinates along each axis."""
+        out = []
+        for a in range(3):
+            n = self._shape[a]
+            out.append(self._pos_c[a] + self._voxwid * (np.arange(n, dtype=np.float32) - (n - 1) / 2))
+        return tuple(out)  # type: ignore[return-value]
+
+    @property
+    def minxyz_maxxyz(self) -> tuple[tuple[float, float, float], tuple[float, float, float]]:
+        """Boundary tuple ((minx,miny,minz),(maxx,maxy,maxz))."""
+        xs, ys, zs = self.xs_ys_zs
+        h = self._voxwid / 2
+        return (
+            (float(xs.min() - h), float(ys.min() - h), float(zs.min() - h)),
+            (float(xs.max() + h), float(ys.max() + h), float(zs.max() + h)),
+        )
+
+    # ------------------------------------------------------------ descriptors
+    def _desc(self) -> np.ndarray:
+        return _lib.vol_desc(self._shape, self._order, self._voxwid, self.corner)
+
+    @property
+    def _numel(self) -> int:
+        return int(np.prod(self._shape))
+
+    # --------------------------------------------------------------- elementwise
+    def fill(self, value: float) -> None:
+        """Fill the volume with a constant value."""
+        _lib.check(
+            _lib.lib().aprict_b200_vol_fill(self._data.data_ptr(), self._numel, float(value), _stream()),
+            "Volume.fill",
+        )
+
+    def multiply(self, f: float) -> None:
+        """Multiply the volume in place by a value."""
+        _lib.check(
+            _lib.lib().aprict_b200_vol_scale(self._data.data_ptr(), self._numel, float(f), _stream()),
+            "Volume.multiply",
+        )
+
+    def invert(self, *, ignore_zeros: bool = False, softmax_epsilon: float | None = None) -> None:
+        """v <- 1/(v + eps exp(-v/eps)) (texture_tools.operations.invert, operations.py:347-374)."""
+        _lib.check(
+            _lib.lib().aprict_b200_vol_invert(
+                self._data.data_ptr(), self._numel, int(bool(ignore_zeros)), float(softmax_epsilon or 0), _stream()
+            ),
+            "Volume.invert",
+        )
+
+    def multiply_volume(self, other: Volume) -> None:
+        """Element-wise product with another volume of the same shape and order."""
+        self._check_same(other)
+        _lib.check(
+            _lib.lib().aprict_b200_vol_mul(
+                self._data.data_ptr(), self._data.data_ptr(), other._data.data_ptr(), self._numel, _stream()
+            ),
+            "Volume.multiply_volume",
+        )
+
+    def add_scaled(self, other: Volume, alpha: float) -> None:
+        """self += alpha * other."""
+        self._check_same(other)
+        _lib.check(
+            _lib.lib().aprict_b200_vol_axpy(
+                self._data.data_ptr(),
+                self._data.data_ptr(),
+                float(alpha),
+                other._data.data_ptr(),
+                self._numel,
+                _stream(),
+            ),
+            "Volume.add_scaled",
+        )
+
+    def inner_product(self, other: Volume) -> float:
+        """<self, other> accumulated in double on the device."""
+        self._check_same(other)
+        out = torch.zeros((), dtype=torch.float64, device=self._data.device)
+        _lib.check(
+            _lib.lib().aprict_b200_vol_dot(
+                self._data.data_ptr(), other._data.data_ptr(), self._numel, out.data_ptr(), _stream()
+            ),
+            "Volume.inner_product",
+        )
+        return float(out.item())
+
+    def soften_to_xy_cylinder(self, relrad_start: float) -> None:
+        """Soft-mask to a cylinder coaxial with the volume's z axis (operations.py:377-401)."""
+        if not 0 <= relrad_start <= 1:
+            msg = "The input 'relrad_start' should be between 0 and 1."
+            raise ValueError(msg)
+        d = self._desc()
+        _lib.check(
+            _lib.lib().aprict_b200_vol_softmask_cylinder(
+                self._data.data_ptr(), _lib.ptr(d), float(relrad_start), _stream()
+            ),
+            "Volume.soften_to_xy_cylinder",
+        )
+
+    def _check_same(self, other: Volume) -> None:
+        if other.shape != self.shape:
+            msg = f"Shape mismatch: {self.shape} vs {other.shape}"
+            raise ValueError(msg)
+        if other.order != self.order:
+            msg = "Volumes of different memory order are not supported in element-wise operations."
+            raise NotImplementedError(msg)
+
+    # ----------------------------------------------------------------- copies
+    def copy_from(self, arr: np.ndarray | torch.Tensor, block: bool = True) -> None:
+        """Copy a host/device array of shape (X,Y,Z) into this volume."""
+        if tuple(arr.shape) != self._shape:
+            msg = f"Shape mismatch: expected {self._shape}, got {tuple(arr.shape)}"
+            raise ValueError(msg)
+        src = arr if isinstance(arr, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32))
+        self._data.copy_(src.to(torch.float32), non_blocking=not block)
+        if block:
+            torch.cuda.current_stream().synchronize()
+
+    def copy_to(self, arr: np.ndarray | torch.Tensor, block: bool = True) -> None:
+        """Copy this volume into a host/device array of shape (X,Y,Z)."""
+        if isinstance(arr, torch.Tensor):
+            arr.copy_(self._data, non_blocking=not block)
+        else:
+            arr[...] = self._data.cpu().numpy()
+        if block:
+            torch.cuda.current_stream().synchronize()
+
+    def as_numpy(self, out: np.ndarray | None = None, allow_indirect_copy: bool = False) -> np.ndarray:  # noqa: ARG002
+        """Copy this volume into a numpy array."""
+        host = self._data.cpu().numpy()
+        if out is None:
+            return np.array(host, order=self._order)
+        out[...] = host
+        return out
+
+    def as_torch(self) -> torch.Tensor:
+        """A device copy of the volume as a torch tensor."""
+        return self._data.clone()
+
+    def as_cupy(self, out: object | None = None) -> object:  # noqa: ARG002
+        """A CuPy view of the data (requires CuPy; zero-copy through DLPack)."""
+        try:
+            import cupy as cp  # noqa: PLC0415
+        except ImportError as e:
+            msg = "as_cupy needs CuPy; use as_torch() or .data instead"
+            raise ImportError(msg) from e
+        return cp.from_dlpack(self._data)
+
+    def save(self, path: pathlib.Path | str) -> None:
+        """Save the volume to a .npy file."""
+        np.save(path, self.as_numpy())
+
+    # ------------------------------------------------------------ constructors
+    @classmethod
+    def zeros(
+        cls,
+        shape: tuple[int, int, int],
+        *,
+        voxwid: float,
+        dtype: type | np.dtype = np.float32,
+        pos_c: np.ndarray | tuple[float, float, float] = (0.0, 0.0, 0.0),
+        initialize_texture: bool = True,
+        order: typing.Literal["C", "F"] = "C",
+    ) -> Volume:
+        """A new zero-filled volume (``initialize_texture=False`` allocates nothing)."""
+        if type(shape) is not tuple or len(shape) != 3:
+            msg = "Invalid shape provided. It should be a tuple of three positive integers."
+            raise ValueError(msg)
+        if np.dtype(dtype) not in _SUPPORTED_DTYPES:
+            msg = f"Volume dtype {np.dtype(dtype)} is not supported (float32 only)."
+            raise NotImplementedError(msg)
+        self = cls.__new__(cls)
+        self._shape = tuple(int(s) for s in shape)  # type: ignore[assignment]
+        self._dtype = np.dtype(dtype)
+        self._order = order
+        self._voxwid = float(voxwid)
+        self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
+        if initialize_texture:
+            self._data = _empty(self._shape, order)
+            self.fill(0.0)
+        return self
+
+    def zeroed_copy(self) -> Volume:
+        """A zero-filled volume with this geometry."""
+        return Volume.zeros(self._shape, voxwid=self._voxwid, dtype=self._dtype, pos_c=self.pos_c, order=self._order)
+
+    def copy(self) -> Volume:
+        """A deep copy."""
+        v = self.zeroed_copy()
+        v._data.copy_(self._data)
+        return v
+
+
+class FBVolume:
+    """A volume given as FORBILD analytic shapes (mirrors volume.py:369-495)."""
+
+    def __init__(self, shapes: np.ndarray) -> None:
+        self.shapes = shapes
+
+    def copy(self) -> FBVolume:
+        """A copy of this phantom."""
+        return FBVolume(self.shapes.copy())
+
+    def superimpose_onto(self, vol: FBVolume) -> FBVolume:
+        """This phantom's shapes drawn after (over) ``vol``'s."""
+        return FBVolume(shapes=np.concatenate((vol.shapes, self.shapes), axis=0))
+
+
+__all__ = ["FBVolume", "Volume"]

@@ -1,0 +1,215 @@
+/*
+ * aprict_b200.h -- C ABI of the B200 (sm_100a) cone-beam projection /
+ * reconstruction kernels.
+ *
+ * Every entry point:
+ *   - takes plain pointers and sizes (device pointers are marked *_dev),
+ *   - enqueues work on the given CUDA stream (NULL = legacy default stream)
+ *     and returns without synchronising,
+ *   - allocates no device memory (the caller owns every buffer),
+ *   - returns an aprict_status (0 = OK) after validating its arguments on the
+ *     host; nothing is launched when the return value is nonzero.
+ *
+ * Operators ACCUMULATE into their output, as the reference's do
+ * (project: atomicAdd in CB_project_texture_chunked.cu:411; backproject:
+ * surface read-modify-write in CB_backproject.cu:1010-1015).
+ *
+ * Data layout (matches the reference's Python API, flatpanel.py:81-83 and
+ * volume.py:133-145):
+ *   - volume (X,Y,Z) float32, C order (z fastest) or F order (x fastest);
+ *     voxel (i,j,k) centre = corner + voxwid*((i,j,k) + 0.5);
+ *   - projections (views, nu, nv) float32 with arbitrary element strides;
+ *     pixel (iu,iv) centre = det_pos + det_u*(iu-(nu-1)/2) + det_v*(iv-(nv-1)/2).
+ */
+#ifndef APRICT_B200_H
+#define APRICT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *aprict_stream_t; /* a cudaStream_t */
+
+#if defined(__GNUC__)
+#define APRICT_API __attribute__((visibility("default")))
+#else
+#define APRICT_API
+#endif
+
+/* Host-side return codes. */
+typedef enum {
+    APRICT_OK = 0,
+    APRICT_ERR_INVALID_ARGUMENT = 1, /* reference: ValueError (flatpanel.py:1141-1159) */
+    APRICT_ERR_UNSUPPORTED = 2,      /* reference: NotImplementedError (flatpanel.py:247-255) */
+    APRICT_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+    APRICT_ERR_TOO_LARGE = 4,        /* a size exceeds what the kernel indexes */
+    APRICT_ERR_NO_DEVICE = 5         /* no usable sm_100 device */
+} aprict_status;
+
+/* Bits of the optional device status word (uint32) a kernel ORs into. */
+#define APRICT_STATUS_OVERFLOW 0x1u     /* quadric interval list full (reference out_of_mem_count) */
+#define APRICT_STATUS_NONFINITE 0x2u    /* a non-finite ray or voxel value was met */
+#define APRICT_STATUS_BAD_GEOMETRY 0x4u /* degenerate view (zero-length detector vectors, ...) */
+#define APRICT_STATUS_TIMEOUT 0x8u      /* a bounded wait gave up */
+
+typedef struct {
+    float x, y, z;
+} aprict_fvec3;
+
+/* One cone-beam view. Byte-identical to the reference's proj_spec
+ * (geometry.h:1-13: fvec3 sourcepos; det_spec{pos,u,v,nu,nv,type}); 60 bytes. */
+typedef struct {
+    aprict_fvec3 source_pos;
+    aprict_fvec3 det_pos; /* centre of the detector */
+    aprict_fvec3 det_u;   /* pixel-centre step along a row (index iu) */
+    aprict_fvec3 det_v;   /* pixel-centre step along a column (index iv) */
+    uint32_t nu;
+    uint32_t nv;
+    uint8_t type; /* 0 = flat panel; anything else is rejected */
+    uint8_t pad_[3];
+} aprict_proj_spec;
+
+/* Voxel grid. Replaces the reference's vol_tex_chunk_spec + surface object
+ * (geometry.h:78-83): a linear device buffer instead of a cudaArray. */
+typedef struct {
+    uint32_t nx, ny, nz;
+    uint32_t order; /* 0 = C order (z fastest), 1 = F order (x fastest) */
+    float voxwid;
+    aprict_fvec3 corner; /* world position of the outer corner of voxel (0,0,0) */
+} aprict_vol_desc;
+
+/* Projection stack (views, nu, nv); strides in ELEMENTS (the reference passes
+ * byte strides as ulvec3(view,u,v), CB_project_texture_chunked.cu:366-370). */
+typedef struct {
+    uint32_t n_views, nu, nv, pad_;
+    int64_t stride_view, stride_u, stride_v;
+} aprict_proj_desc;
+
+/* Same fields and layout as the reference's config_CB_project
+ * (config_cb_project.h / geometry.h:94-99). */
+typedef struct {
+    float shrink_volume_factor;
+    float multiply_before_adding;
+    uint32_t ssu, ssv;
+} aprict_project_config;
+
+/* Fields of the reference's config_CB_backproject (geometry.h:108-128),
+ * widened to 32-bit members. */
+typedef struct {
+    uint32_t exact;              /* exact_line_integ_backproj */
+    uint32_t backproject_all_1s; /* exact mode only, as in the reference */
+    uint32_t mask_to_cylinder;
+    float mask_to_cyl_rad; /* world units, cylinder about world x=y=0 */
+    uint32_t apply_summand_multiplier;
+    float soften_edge_proportion;
+    int32_t Z_on_L_factor_power;
+    int32_t Z_on_val_factor_power;
+    float Z_on_val_factor_val;
+    uint32_t approx_mode_direct_raycast;
+    uint32_t approx_mode_linear_interpolate;
+    uint32_t weighting_preset; /* only 0 is implemented */
+    uint32_t ssx, ssy, ssz;
+    float soft_vartheta_v, soft_vartheta_v_softspan;
+    float soft_vartheta_h, soft_vartheta_h_softspan;
+} aprict_backproject_config;
+
+/* Human-readable text for an aprict_status code. */
+APRICT_API const char *aprict_b200_status_string(int status);
+
+/* Detail of the last nonzero status returned on the calling host thread. */
+APRICT_API const char *aprict_b200_last_error(void);
+
+/* Library version as "MAJOR.MINOR.PATCH". */
+APRICT_API const char *aprict_b200_version(void);
+
+/* sizeof() of a struct declared here, by its type name (0 if unknown); lets
+ * bindings verify their struct mirrors without a GPU. */
+APRICT_API size_t aprict_b200_struct_size(const char *name);
+
+/* Siddon exact line-integral forward projection of a voxel volume.
+ * Replaces project_CB_texture_chunked<float,float>
+ * (CB_project_texture_chunked.cu:327-412) as launched by
+ * flatpanel.project (flatpanel.py:997-1125).
+ *   specs_dev : n_views aprict_proj_spec in device memory
+ *   base_dev  : NULL  -> projs += mba * A vol   (reference semantics, atomic)
+ *               !NULL -> projs  = base + mba * A vol (fused residual; base may
+ *                        equal projs_dev; same strides as projs)
+ *   status_dev: optional device word (may be NULL)                        */
+APRICT_API int aprict_b200_project_siddon(const aprict_proj_spec *specs_dev,
+                               const aprict_proj_desc *projs, float *projs_dev,
+                               const float *base_dev,
+                               const aprict_vol_desc *vol, const float *vol_dev,
+                               const aprict_project_config *cfg,
+                               uint32_t *status_dev, aprict_stream_t stream);
+
+/* Ray-driven matched adjoint of aprict_b200_project_siddon:
+ * vol += A^T projs with exactly the forward projector's intersection lengths
+ * (the same traversal code), scattered with atomic adds. No counterpart
+ * kernel in the reference; it is the transpose the reference's exact
+ * backprojector (CB_backproject.cu:408-477) approximates voxel by voxel. */
+APRICT_API int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev,
+                                    const aprict_proj_desc *projs,
+                                    const float *projs_dev,
+                                    const aprict_vol_desc *vol, float *vol_dev,
+                                    const aprict_project_config *cfg,
+                                    uint32_t *status_dev,
+                                    aprict_stream_t stream);
+
+/* Voxel-driven backprojection (exact chord-length footprint or fast
+ * nearest/bilinear), all views in one launch:
+ * vol += multiplier * BP(projs). Replaces backproject_CB_voltex<float,float>
+ * (CB_backproject.cu:952-1027, per-voxel body :313-733) and the host loop of
+ * 10-view launches in flatpanel.backproject (flatpanel.py:1128-1281).
+ *   multiplier_dev: required iff cfg->apply_summand_multiplier (same layout
+ *                   as vol)                                               */
+APRICT_API int aprict_b200_backproject(const aprict_proj_spec *specs_dev,
+                            const aprict_proj_desc *projs,
+                            const float *projs_dev,
+                            const aprict_vol_desc *vol, float *vol_dev,
+                            const float *multiplier_dev,
+                            const aprict_backproject_config *cfg,
+                            uint32_t *status_dev, aprict_stream_t stream);
+
+
+/* ---- Element-wise volume operations (linear float32 buffers of n elements).
+ * Replace the surface kernels of texture_operations.cu driven by
+ * src/aprict/lib/texture_tools/operations.py. ---- */
+
+/* v[:] = value (fill_surface, texture_operations.cu:124-135). */
+APRICT_API int aprict_b200_vol_fill(float *v_dev, int64_t n, float value, aprict_stream_t stream);
+
+/* v *= factor (multiply_surface, texture_operations.cu:187-199). */
+APRICT_API int aprict_b200_vol_scale(float *v_dev, int64_t n, float factor, aprict_stream_t stream);
+
+/* v <- 1/(v + eps*exp(-v/eps)) (eps > 0) or 1/v (eps == 0), zeros kept when
+ * ignore_zeros (multiplicatively_invert_surface, texture_operations.cu:164-185). */
+APRICT_API int aprict_b200_vol_invert(float *v_dev, int64_t n, int ignore_zeros, float eps,
+                                      aprict_stream_t stream);
+
+/* Cosine taper outside relrad_start of the inscribed xy circle about the
+ * volume centre; relrad_start == 1 zeroes everything outside the circle
+ * (softmask_surface_to_cylinder_xy, texture_operations.cu:137-162). */
+APRICT_API int aprict_b200_vol_softmask_cylinder(float *v_dev, const aprict_vol_desc *vol,
+                                                 float relrad_start, aprict_stream_t stream);
+
+/* *out_dev += sum(a*b), accumulated in double (inner_product_3D_surfaces,
+ * texture_operations.cu:284-307). The caller zeroes *out_dev. */
+APRICT_API int aprict_b200_vol_dot(const float *a_dev, const float *b_dev, int64_t n, double *out_dev,
+                                   aprict_stream_t stream);
+
+/* out = a * b element-wise (multiply_surfaces, texture_operations.cu:309-). */
+APRICT_API int aprict_b200_vol_mul(float *out_dev, const float *a_dev, const float *b_dev, int64_t n,
+                                   aprict_stream_t stream);
+
+/* out = a + alpha * b element-wise (out may alias a). */
+APRICT_API int aprict_b200_vol_axpy(float *out_dev, const float *a_dev, float alpha, const float *b_dev,
+                                    int64_t n, aprict_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APRICT_B200_H */

@@ -1,0 +1,404 @@
+/* ab_oracle.c -- FP64 CPU restatement of the reference's projection and
+ * backprojection arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY. The checker for the CUDA kernels: tests/,
+ * __graft_entry__.smoke() and bench.py's CPU baseline load it; the
+ * aprict_b200 package never does.
+ *
+ * The line integral is the one exact_line_integral_unitvoxwid computes
+ * (src/aprict/data/cusrc/CB_project_texture_chunked.cu:111-306), restated as
+ * Siddon's original parametric form: all voxel-boundary crossings along the
+ * source->pixel segment are generated in order, and each piece between two
+ * consecutive crossings is charged to the voxel containing its midpoint. Every
+ * quantity is double; nothing is stepped incrementally. Tie rules follow the
+ * reference: with a zero direction component the voxel along that axis is
+ * ceil(c)-1 (reference :189-203, :244-246).
+ *
+ * The voxel-driven backprojector follows _backproject_CB_getval
+ * (src/aprict/data/cusrc/CB_backproject.cu:313-733) for weighting preset 0.
+ */
+#include "ab_oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    double x, y, z;
+} d3;
+
+static d3 d3f(ao_fvec3 v) { return (d3){v.x, v.y, v.z}; }
+static d3 add(d3 a, d3 b) { return (d3){a.x + b.x, a.y + b.y, a.z + b.z}; }
+static d3 sub(d3 a, d3 b) { return (d3){a.x - b.x, a.y - b.y, a.z - b.z}; }
+static d3 scl(d3 a, double s) { return (d3){a.x * s, a.y * s, a.z * s}; }
+static double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static double nrm(d3 a) { return sqrt(dot(a, a)); }
+static d3 cross(d3 a, d3 b) { return (d3){a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+static int64_t vidx(const ao_grid *g, int ix, int iy, int iz) {
+    if (g->order == 0) return ((int64_t)ix * g->ny + iy) * g->nz + iz;
+    return ((int64_t)iz * g->ny + iy) * g->nx + ix;
+}
+
+/* Pixel (fractional index fu, fv) centre in world units. */
+static d3 pixel_pos(const ao_proj_spec *sp, double fu, double fv) {
+    const double xn = fu - ((double)sp->nu - 1.0) * 0.5;
+    const double yn = fv - ((double)sp->nv - 1.0) * 0.5;
+    return add(d3f(sp->det_pos), add(scl(d3f(sp->det_u), xn), scl(d3f(sp->det_v), yn)));
+}
+
+typedef void (*visit_fn)(void *ctx, double seg, int ix, int iy, int iz);
+
+/* Visits every piece of the ray o + a (e - o), a in [0, a_max], inside the
+ * grid [0,n)^3 (voxel units). Returns |e - o| (0 if the ray misses). */
+static double traverse(const double o[3], const double e[3], const int n[3], double a_max, visit_fn f, void *ctx) {
+    double d[3], a_in = 0.0, a_out = a_max;
+    for (int a = 0; a < 3; ++a) {
+        d[a] = e[a] - o[a];
+        if (d[a] == 0.0) {
+            if (!(o[a] > 0.0 && o[a] <= (double)n[a])) return 0.0;
+        } else {
+            const double t0 = (0.0 - o[a]) / d[a], t1 = ((double)n[a] - o[a]) / d[a];
+            const double lo = t0 < t1 ? t0 : t1, hi = t0 < t1 ? t1 : t0;
+            if (lo > a_in) a_in = lo;
+            if (hi < a_out) a_out = hi;
+        }
+    }
+    const double len = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    if (!(a_in < a_out)) return 0.0;
+    double nxt[3];
+    double bnd[3];
+    int fixed[3];
+    for (int a = 0; a < 3; ++a) {
+        if (d[a] == 0.0) {
+            nxt[a] = INFINITY;
+            bnd[a] = 0.0;
+            fixed[a] = (int)ceil(o[a]) - 1;
+        } else {
+            const double p = o[a] + a_in * d[a];
+            bnd[a] = d[a] > 0.0 ? floor(p) + 1.0 : ceil(p) - 1.0;
+            nxt[a] = (bnd[a] - o[a]) / d[a];
+            fixed[a] = 0;
+        }
+    }
+    double prev = a_in;
+    for (;;) {
+        double t = a_out;
+        for (int a = 0; a < 3; ++a)
+            if (nxt[a] < t) t = nxt[a];
+        if (t > prev) {
+            const double mid = 0.5 * (prev + t);
+            int idx[3];
+            for (int a = 0; a < 3; ++a) {
+                idx[a] = d[a] == 0.0 ? fixed[a] : (int)floor(o[a] + mid * d[a]);
+                if (idx[a] < 0) idx[a] = 0;
+                if (idx[a] >= n[a]) idx[a] = n[a] - 1;
+            }
+            f(ctx, t - prev, idx[0], idx[1], idx[2]);
+        }
+        if (t >= a_out) break;
+        for (int a = 0; a < 3; ++a) {
+            if (nxt[a] <= t) {
+                bnd[a] += d[a] > 0.0 ? 1.0 : -1.0;
+                nxt[a] = (bnd[a] - o[a]) / d[a];
+            }
+        }
+        prev = t;
+    }
+    return len;
+}
+
+typedef struct {
+    const float *vol;
+    const ao_grid *g;
+    double acc;
+    int64_t nseg;
+} gather_ctx;
+
+static void gather_visit(void *c, double seg, int ix, int iy, int iz) {
+    gather_ctx *x = (gather_ctx *)c;
+    x->acc += seg * (double)x->vol[vidx(x->g, ix, iy, iz)];
+    x->nseg++;
+}
+
+static void to_grid(const ao_grid *g, d3 p, double out[3]) {
+    out[0] = (p.x - g->corner[0]) / g->voxwid;
+    out[1] = (p.y - g->corner[1]) / g->voxwid;
+    out[2] = (p.z - g->corner[2]) / g->voxwid;
+}
+
+void ao_project_siddon(const ao_proj_spec *specs, int n_views, int nu, int nv, const float *vol, const ao_grid *g,
+                       double svf, double mba, int ssu, int ssv, double *out, int64_t *nseg, int nthreads) {
+    const int n[3] = {g->nx, g->ny, g->nz};
+    int64_t total = 0;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for collapse(2) schedule(dynamic, 4) reduction(+ : total)
+    for (int m = 0; m < n_views; ++m) {
+        for (int iu = 0; iu < nu; ++iu) {
+            const ao_proj_spec *sp = &specs[m];
+            double o[3];
+            to_grid(g, scl(d3f(sp->source_pos), svf), o);
+            for (int iv = 0; iv < nv; ++iv) {
+                double tot = 0.0;
+                for (int ku = 0; ku < ssu; ++ku) {
+                    double accu = 0.0;
+                    for (int kv = 0; kv < ssv; ++kv) {
+                        const double fu = iu - 0.5 + (ku + 0.5) / ssu, fv = iv - 0.5 + (kv + 0.5) / ssv;
+                        double e[3];
+                        to_grid(g, scl(pixel_pos(sp, fu, fv), svf), e);
+                        gather_ctx c = {vol, g, 0.0, 0};
+                        const double len = traverse(o, e, n, 1.0, gather_visit, &c);
+                        accu += mba * g->voxwid * len * c.acc;
+                        total += c.nseg;
+                    }
+                    tot += accu / ssv;
+                }
+                out[((int64_t)m * nu + iu) * nv + iv] += tot / ssu;
+            }
+        }
+    }
+    if (nseg) *nseg = total;
+}
+
+typedef struct {
+    double *vol;
+    const ao_grid *g;
+    double w;
+} scatter_ctx;
+
+static void scatter_visit(void *c, double seg, int ix, int iy, int iz) {
+    scatter_ctx *x = (scatter_ctx *)c;
+    x->vol[vidx(x->g, ix, iy, iz)] += seg * x->w;
+}
+
+static double *alloc_private(int nthr, int64_t nvox) {
+    return (double *)calloc((size_t)nthr * (size_t)nvox, sizeof(double));
+}
+
+void ao_backproject_transpose(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
+                              const ao_grid *g, double svf, double mba, int ssu, int ssv, double *vol,
+                              int nthreads) {
+    const int n[3] = {g->nx, g->ny, g->nz};
+    const int64_t nvox = (int64_t)g->nx * g->ny * g->nz;
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const int nthr = omp_get_max_threads();
+    double *priv = alloc_private(nthr, nvox);
+#pragma omp parallel
+    {
+        double *mine = priv + (int64_t)omp_get_thread_num() * nvox;
+#pragma omp for collapse(2) schedule(dynamic, 4)
+        for (int m = 0; m < n_views; ++m) {
+            for (int iu = 0; iu < nu; ++iu) {
+                const ao_proj_spec *sp = &specs[m];
+                double o[3];
+                to_grid(g, scl(d3f(sp->source_pos), svf), o);
+                for (int iv = 0; iv < nv; ++iv) {
+                    const double p = projs[((int64_t)m * nu + iu) * nv + iv];
+                    if (p == 0.0) continue;
+                    for (int ku = 0; ku < ssu; ++ku) {
+                        for (int kv = 0; kv < ssv; ++kv) {
+                            const double fu = iu - 0.5 + (ku + 0.5) / ssu, fv = iv - 0.5 + (kv + 0.5) / ssv;
+                            double e[3];
+                            to_grid(g, scl(pixel_pos(sp, fu, fv), svf), e);
+                            const double dd[3] = {e[0] - o[0], e[1] - o[1], e[2] - o[2]};
+                            const double len = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+                            scatter_ctx c = {mine, g, p * mba * g->voxwid * len / (ssu * ssv)};
+                            traverse(o, e, n, 1.0, scatter_visit, &c);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    for (int t = 0; t < nthr; ++t) {
+        const double *src = priv + (int64_t)t * nvox;
+        for (int64_t i = 0; i < nvox; ++i) vol[i] += src[i];
+    }
+    free(priv);
+}
+
+/* ---- voxel-driven backprojection (CB_backproject.cu:313-733) ---- */
+
+static double powint(double b, int e) {
+    double a = 1.0;
+    if (e < 0)
+        for (int k = 0; k < -e; ++k) a /= b;
+    else
+        for (int k = 0; k < e; ++k) a *= b;
+    return a;
+}
+
+/* get_projected_detector_coords (geometry.h:24-56), FP64: coordinates from the
+ * detector centre in pixels. */
+static void det_coords(const ao_proj_spec *sp, d3 x, double *cu, double *cv) {
+    const d3 s = d3f(sp->source_pos), P = d3f(sp->det_pos), U = d3f(sp->det_u), V = d3f(sp->det_v);
+    const d3 n = cross(U, V);
+    d3 p = add(s, scl(sub(x, s), dot(sub(P, s), n) / dot(sub(x, s), n)));
+    p = sub(p, P);
+    *cu = dot(U, p) / dot(U, U);
+    *cv = dot(V, p) / dot(V, V);
+}
+
+static double get2d(const double *img, int nu, int nv, int i, int j) {
+    if (i < 0 || i >= nu || j < 0 || j >= nv) return 0.0;
+    return img[(int64_t)i * nv + j];
+}
+
+static double taper(double cu, double cv, int nu, int nv, double sep) {
+    double ud = fabs(cu) / (nu / 2.0), vd = fabs(cv) / (nv / 2.0);
+    ud = fmax(0.0, fmin(1.0, (1.0 - ud) / sep));
+    vd = fmax(0.0, fmin(1.0, (1.0 - vd) / sep));
+    ud = fmax(0.0, fmin(1.0, (1.0 + cos(M_PI * (1.0 - ud))) / 2.0));
+    vd = fmax(0.0, fmin(1.0, (1.0 + cos(M_PI * (1.0 - vd))) / 2.0));
+    return ud * vd;
+}
+
+static d3 voxel_centre(const ao_grid *g, int ix, int iy, int iz) {
+    return (d3){g->corner[0] + (ix + 0.5) * g->voxwid, g->corner[1] + (iy + 0.5) * g->voxwid,
+                g->corner[2] + (iz + 0.5) * g->voxwid};
+}
+
+/* Value one (sub-)voxel at x receives from view m in fast mode. */
+static double fast_value(const ao_proj_spec *sp, const double *img, d3 x, double voxwid, const ao_bp_cfg *c) {
+    const d3 s = d3f(sp->source_pos), P = d3f(sp->det_pos), U = d3f(sp->det_u), V = d3f(sp->det_v);
+    const int nu = (int)sp->nu, nv = (int)sp->nv;
+    double cu, cv;
+    det_coords(sp, x, &cu, &cv);
+    const double fu = cu + (nu - 1) / 2.0, fv = cv + (nv - 1) / 2.0;
+    const d3 L = sub(P, s);
+    double mult, value;
+    double pv;
+    if (c->linear) {
+        if (fu <= -1 || fv <= -1 || fu >= nu || fv >= nv) {
+            pv = 0.0;
+        } else {
+            const int i0 = (int)floor(fu), j0 = (int)floor(fv);
+            const double fx = fu - i0, fy = fv - j0;
+            const double t1 = get2d(img, nu, nv, i0, j0) * (1 - fx) + get2d(img, nu, nv, i0 + 1, j0) * fx;
+            const double t2 = get2d(img, nu, nv, i0, j0 + 1) * (1 - fx) + get2d(img, nu, nv, i0 + 1, j0 + 1) * fx;
+            pv = t1 * (1 - fy) + t2 * fy;
+        }
+    } else {
+        pv = get2d(img, nu, nv, (int)floor(fu + 0.5), (int)floor(fv + 0.5));
+    }
+    if (c->raycast) {
+        mult = 1.0;
+        const double Z = dot(sub(x, s), L) / nrm(L);
+        if (c->pL) mult *= powint(Z / nrm(L), c->pL);
+        if (c->pV) mult *= powint(Z / c->val, c->pV);
+        value = pv * mult;
+    } else {
+        const d3 detp = add(P, add(scl(U, cu), scl(V, cv)));
+        const double mag = nrm(sub(detp, s)) / nrm(sub(x, s)) * voxwid;
+        mult = mag * mag / (nrm(U) * nrm(V));
+        if (c->pL) mult *= powint(dot(sub(x, s), L) / dot(L, L), c->pL);
+        if (c->pV) mult *= powint(dot(scl(sub(x, s), 1.0 / c->val), L) / nrm(L), c->pV);
+        value = voxwid * pv * mult;
+    }
+    if (c->sep > 0 && value != 0.0) value *= taper(cu, cv, nu, nv, c->sep);
+    return value;
+}
+
+static int masked(const ao_grid *g, const ao_bp_cfg *c, int ix, int iy, int iz) {
+    if (!c->mask) return 0;
+    const d3 x = voxel_centre(g, ix, iy, iz);
+    return x.x * x.x + x.y * x.y > c->mask_rad * c->mask_rad;
+}
+
+void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
+                    const ao_grid *g, const double *mult, const ao_bp_cfg *c, double *vol, int nthreads) {
+    const int64_t nvox = (int64_t)g->nx * g->ny * g->nz;
+    const int64_t img = (int64_t)nu * nv;
+    const double inv_ss = 1.0 / ((double)c->ssx * c->ssy * c->ssz);
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    if (!c->exact) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 2)
+        for (int ix = 0; ix < g->nx; ++ix) {
+            for (int iy = 0; iy < g->ny; ++iy) {
+                for (int iz = 0; iz < g->nz; ++iz) {
+                    if (masked(g, c, ix, iy, iz)) continue;
+                    const d3 xc = voxel_centre(g, ix, iy, iz);
+                    double acc = 0.0;
+                    for (int si = 0; si < c->ssx; ++si)
+                        for (int sj = 0; sj < c->ssy; ++sj)
+                            for (int sk = 0; sk < c->ssz; ++sk) {
+                                const d3 x = add(xc, scl((d3){-0.5 + (si + 0.5) / c->ssx, -0.5 + (sj + 0.5) / c->ssy,
+                                                              -0.5 + (sk + 0.5) / c->ssz},
+                                                         g->voxwid));
+                                for (int m = 0; m < n_views; ++m)
+                                    acc += fast_value(&specs[m], projs + m * img, x, g->voxwid, c);
+                            }
+                    const int64_t o = vidx(g, ix, iy, iz);
+                    vol[o] += acc * inv_ss * (mult ? mult[o] : 1.0);
+                }
+            }
+        }
+        return;
+    }
+    /* Exact mode: sum over footprint pixels of value * chord(pixel-centre ray,
+     * voxel cube) (:408-477) == per view, the transpose of a pixel-centre-ray
+     * projection over the voxel grid (rays from the source, unbounded past the
+     * detector as the reference's chord is), times the per-voxel weights. */
+    const int nthr = omp_get_max_threads();
+    double *priv = alloc_private(nthr, nvox);
+    double *tmp = alloc_private(nthr, nvox);
+    const int n[3] = {g->nx, g->ny, g->nz};
+#pragma omp parallel
+    {
+        double *acc = priv + (int64_t)omp_get_thread_num() * nvox;
+        double *T = tmp + (int64_t)omp_get_thread_num() * nvox;
+#pragma omp for schedule(dynamic, 1)
+        for (int m = 0; m < n_views; ++m) {
+            const ao_proj_spec *sp = &specs[m];
+            const d3 s = d3f(sp->source_pos), L = sub(d3f(sp->det_pos), s);
+            for (int si = 0; si < c->ssx; ++si)
+                for (int sj = 0; sj < c->ssy; ++sj)
+                    for (int sk = 0; sk < c->ssz; ++sk) {
+                        const d3 off = scl((d3){-0.5 + (si + 0.5) / c->ssx, -0.5 + (sj + 0.5) / c->ssy,
+                                                -0.5 + (sk + 0.5) / c->ssz},
+                                           g->voxwid);
+                        ao_grid gs = *g;
+                        gs.corner[0] += off.x;
+                        gs.corner[1] += off.y;
+                        gs.corner[2] += off.z;
+                        memset(T, 0, sizeof(double) * (size_t)nvox);
+                        double o[3];
+                        to_grid(&gs, s, o);
+                        for (int iu = 0; iu < nu; ++iu)
+                            for (int iv = 0; iv < nv; ++iv) {
+                                const double p = c->all_ones ? 1.0 : projs[m * img + (int64_t)iu * nv + iv];
+                                if (p == 0.0) continue;
+                                double e[3];
+                                to_grid(&gs, pixel_pos(sp, iu, iv), e);
+                                const double dd[3] = {e[0] - o[0], e[1] - o[1], e[2] - o[2]};
+                                const double len = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+                                scatter_ctx sc = {T, &gs, p * len * g->voxwid};
+                                traverse(o, e, n, INFINITY, scatter_visit, &sc);
+                            }
+                        for (int ix = 0; ix < g->nx; ++ix)
+                            for (int iy = 0; iy < g->ny; ++iy)
+                                for (int iz = 0; iz < g->nz; ++iz) {
+                                    const int64_t i = vidx(g, ix, iy, iz);
+                                    if (T[i] == 0.0 || masked(g, c, ix, iy, iz)) continue;
+                                    const d3 x = add(voxel_centre(g, ix, iy, iz), off);
+                                    double w = 1.0;
+                                    if (c->pL) w *= powint(dot(sub(x, s), L) / dot(L, L), c->pL);
+                                    if (c->pV) w *= powint(dot(scl(sub(x, s), 1.0 / c->val), L) / nrm(L), c->pV);
+                                    if (c->sep > 0) {
+                                        double cu, cv;
+                                        det_coords(sp, x, &cu, &cv);
+                                        w *= taper(cu, cv, nu, nv, c->sep);
+                                    }
+                                    acc[i] += T[i] * w * inv_ss;
+                                }
+                    }
+        }
+    }
+    for (int t = 0; t < nthr; ++t) {
+        const double *src = priv + (int64_t)t * nvox;
+        for (int64_t i = 0; i < nvox; ++i) vol[i] += src[i] * (mult ? mult[i] : 1.0);
+    }
+    free(priv);
+    free(tmp);
+}

@@ -1,0 +1,52 @@
+/* ab_oracle.h -- FP64 CPU restatement of the reference's projection /
+ * backprojection arithmetic. TEST INFRASTRUCTURE ONLY: used by tests/,
+ * __graft_entry__.smoke() and bench.py's CPU baseline as the checker; the
+ * aprict_b200 package never loads it. */
+#ifndef AB_ORACLE_H
+#define AB_ORACLE_H
+#include <stdint.h>
+
+typedef struct {
+    float x, y, z;
+} ao_fvec3;
+
+/* Same 60-byte layout as the reference's proj_spec (geometry.h:1-13). */
+typedef struct {
+    ao_fvec3 source_pos, det_pos, det_u, det_v;
+    uint32_t nu, nv;
+    uint8_t type, pad_[3];
+} ao_proj_spec;
+
+typedef struct {
+    int nx, ny, nz;
+    int order; /* 0 = C (z fastest), 1 = F (x fastest) */
+    double voxwid;
+    double corner[3];
+} ao_grid;
+
+typedef struct {
+    int exact, all_ones, mask;
+    double mask_rad, sep;
+    int pL, pV;
+    double val;
+    int raycast, linear;
+    int ssx, ssy, ssz;
+} ao_bp_cfg;
+
+/* out[m,iu,iv] += mba * line integrals (ssu x ssv sub-rays averaged),
+ * following project_CB_texture_chunked (CB_project_texture_chunked.cu:327-412).
+ * nseg (optional) receives the number of positive-length ray/voxel segments. */
+void ao_project_siddon(const ao_proj_spec *specs, int n_views, int nu, int nv, const float *vol, const ao_grid *g,
+                       double svf, double mba, int ssu, int ssv, double *out, int64_t *nseg, int nthreads);
+
+/* vol += A^T projs for the operator above (exact transpose, FP64). */
+void ao_backproject_transpose(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
+                              const ao_grid *g, double svf, double mba, int ssu, int ssv, double *vol,
+                              int nthreads);
+
+/* vol += mult * BP(projs), the voxel-driven backprojector of
+ * _backproject_CB_getval (CB_backproject.cu:313-733), preset 0, in FP64. */
+void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
+                    const ao_grid *g, const double *mult, const ao_bp_cfg *cfg, double *vol, int nthreads);
+
+#endif

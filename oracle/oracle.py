@@ -1,0 +1,305 @@
+"""ctypes front for the parity oracles.
+
+TEST INFRASTRUCTURE ONLY -- the checker. Imported by tests/, by
+__graft_entry__.smoke() and by bench.py's CPU-baseline / reference arm; the
+aprict_b200 package never imports it and no product path calls it.
+
+Two libraries, both built by oracle/Makefile:
+  * liboracle.so -- our FP64 restatement of the reference's arithmetic
+    (ab_oracle.c; citations there);
+  * _ref/libaprict_ref.so -- the reference's own device code
+    (src/aprict/data/cusrc/CB_project_texture_chunked.cu, CB_backproject.cu,
+    FORBILD_volumes.h) compiled for the CPU in place from the reference
+    checkout. It exists only where the reference sources were present at build
+    time; ``have_ref()`` says whether it was built.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libaprict_ref.so"
+REF_DIR_DEFAULT = pathlib.Path("/root/reference")
+
+proj_spec = np.dtype(
+    {
+        "names": ["source_pos", "det_pos", "det_u", "det_v", "nu", "nv", "type"],
+        "formats": [np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4")])] * 4 + ["<u4", "<u4", "u1"],
+        "offsets": [0, 12, 24, 36, 48, 52, 56],
+        "itemsize": 60,
+    }
+)
+
+
+class AoGrid(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int),
+        ("ny", ctypes.c_int),
+        ("nz", ctypes.c_int),
+        ("order", ctypes.c_int),
+        ("voxwid", ctypes.c_double),
+        ("corner", ctypes.c_double * 3),
+    ]
+
+
+class AoBpCfg(ctypes.Structure):
+    _fields_ = [
+        ("exact", ctypes.c_int),
+        ("all_ones", ctypes.c_int),
+        ("mask", ctypes.c_int),
+        ("mask_rad", ctypes.c_double),
+        ("sep", ctypes.c_double),
+        ("pL", ctypes.c_int),
+        ("pV", ctypes.c_int),
+        ("val", ctypes.c_double),
+        ("raycast", ctypes.c_int),
+        ("linear", ctypes.c_int),
+        ("ssx", ctypes.c_int),
+        ("ssy", ctypes.c_int),
+        ("ssz", ctypes.c_int),
+    ]
+
+
+def build(ref_dir: pathlib.Path | str | None = None, *, quiet: bool = True) -> None:
+    """Build liboracle.so, and _ref/libaprict_ref.so when the reference sources exist."""
+    ref = pathlib.Path(ref_dir) if ref_dir is not None else REF_DIR_DEFAULT
+    targets = ["liboracle.so"]
+    if (ref / "src/aprict/data/cusrc").is_dir():
+        targets.append("ref")
+    out = subprocess.run(
+        ["make", "-C", str(HERE), f"REF={ref}", *targets],
+        capture_output=True,
+        text=True,
+        check=False,
+    )
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+_so: dict[str, ctypes.CDLL] = {}
+
+
+def _load(path: pathlib.Path) -> ctypes.CDLL:
+    key = str(path)
+    if key not in _so:
+        if not path.exists():
+            msg = f"{path} is not built (run `make -C oracle`)"
+            raise RuntimeError(msg)
+        _so[key] = ctypes.CDLL(key)
+    return _so[key]
+
+
+def have_ref() -> bool:
+    """Whether the reference-compiled library is available."""
+    return REF_SO.exists()
+
+
+def nthreads_default() -> int:
+    return int(os.environ.get("APRICT_ORACLE_THREADS", "0")) or (os.cpu_count() or 1)
+
+
+def _p(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def grid(shape: tuple[int, int, int], voxwid: float, corner: np.ndarray, order: str = "C") -> AoGrid:
+    g = AoGrid()
+    g.nx, g.ny, g.nz = (int(s) for s in shape)
+    g.order = 0 if order == "C" else 1
+    g.voxwid = float(np.float32(voxwid))
+    for i in range(3):
+        g.corner[i] = float(np.float32(corner[i]))
+    return g
+
+
+def _specs(specs: np.ndarray) -> np.ndarray:
+    s = np.ascontiguousarray(specs.reshape(-1))
+    if s.dtype.itemsize != 60:
+        msg = "specs must be 60-byte proj_spec records"
+        raise ValueError(msg)
+    return s
+
+
+def _vol_flat(vol: np.ndarray, order: str) -> np.ndarray:
+    return np.ascontiguousarray(vol.astype(np.float32)) if order == "C" else np.asfortranarray(vol.astype(np.float32))
+
+
+# ----------------------------------------------------------------------- FP64 oracle
+def project_siddon(
+    specs: np.ndarray,
+    vol: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    order: str = "C",
+    svf: float = 1.0,
+    mba: float = 1.0,
+    ssu: int = 1,
+    ssv: int = 1,
+    nthreads: int | None = None,
+) -> tuple[np.ndarray, int]:
+    """FP64 Siddon projection; returns (out (M,nu,nv) float64, number of ray-voxel segments)."""
+    lib = _load(ORACLE_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    v = _vol_flat(vol, order)
+    out = np.zeros((m, nu, nv), dtype=np.float64)
+    nseg = ctypes.c_int64(0)
+    g = grid(vol.shape, voxwid, corner, order)
+    lib.ao_project_siddon(
+        _p(s), m, nu, nv, _p(v), ctypes.byref(g), ctypes.c_double(svf), ctypes.c_double(mba), ssu, ssv, _p(out),
+        ctypes.byref(nseg), nthreads or nthreads_default(),
+    )
+    return out, int(nseg.value)
+
+
+def backproject_transpose(
+    specs: np.ndarray,
+    projs: np.ndarray,
+    shape: tuple[int, int, int],
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    order: str = "C",
+    svf: float = 1.0,
+    mba: float = 1.0,
+    ssu: int = 1,
+    ssv: int = 1,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """FP64 transpose of :func:`project_siddon` (returns a volume in ``order``)."""
+    lib = _load(ORACLE_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    p = np.ascontiguousarray(projs, dtype=np.float64)
+    out = np.zeros(shape, dtype=np.float64, order=order)
+    g = grid(shape, voxwid, corner, order)
+    lib.ao_backproject_transpose(
+        _p(s), m, nu, nv, _p(p), ctypes.byref(g), ctypes.c_double(svf), ctypes.c_double(mba), ssu, ssv, _p(out),
+        nthreads or nthreads_default(),
+    )
+    return out
+
+
+def bp_cfg_from_contents(c: np.ndarray) -> AoBpCfg:
+    """Oracle config from a packed aprict_backproject_config record."""
+    k = AoBpCfg()
+    k.exact = int(c["exact"])
+    k.all_ones = int(c["backproject_all_1s"])
+    k.mask = int(c["mask_to_cylinder"])
+    k.mask_rad = float(c["mask_to_cyl_rad"])
+    k.sep = float(c["soften_edge_proportion"])
+    k.pL = int(c["Z_on_L_factor_power"])
+    k.pV = int(c["Z_on_val_factor_power"])
+    k.val = float(c["Z_on_val_factor_val"])
+    k.raycast = int(c["approx_mode_direct_raycast"])
+    k.linear = int(c["approx_mode_linear_interpolate"])
+    k.ssx, k.ssy, k.ssz = int(c["ssx"]), int(c["ssy"]), int(c["ssz"])
+    return k
+
+
+def backproject(
+    specs: np.ndarray,
+    projs: np.ndarray,
+    shape: tuple[int, int, int],
+    cfg_contents: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    order: str = "C",
+    mult: np.ndarray | None = None,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """FP64 voxel-driven backprojection (returns the increment, a volume in ``order``)."""
+    lib = _load(ORACLE_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    p = np.ascontiguousarray(projs, dtype=np.float64)
+    out = np.zeros(shape, dtype=np.float64, order=order)
+    g = grid(shape, voxwid, corner, order)
+    k = bp_cfg_from_contents(cfg_contents)
+    mm = None if mult is None else np.asarray(mult, dtype=np.float64, order=order)
+    lib.ao_backproject(
+        _p(s), m, nu, nv, _p(p), ctypes.byref(g), None if mm is None else _p(mm), ctypes.byref(k), _p(out),
+        nthreads or nthreads_default(),
+    )
+    return out
+
+
+# ------------------------------------------------------- reference compiled for the CPU
+def ref_project_siddon(
+    specs: np.ndarray,
+    vol: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    svf: float = 1.0,
+    mba: float = 1.0,
+    ssu: int = 1,
+    ssv: int = 1,
+    out: np.ndarray | None = None,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """The reference's project_CB_texture_chunked<float,float> run on the CPU (C-order volume)."""
+    lib = _load(REF_SO)
+    lib.ref_project_siddon.restype = ctypes.c_longlong
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    v = np.ascontiguousarray(vol, dtype=np.float32)
+    o = np.zeros((m, nu, nv), dtype=np.float32) if out is None else out
+    tp = np.asarray(corner, dtype=np.float32)
+    oob = lib.ref_project_siddon(
+        _p(s), m, nu, nv, _p(v), vol.shape[0], vol.shape[1], vol.shape[2], ctypes.c_float(voxwid), _p(tp),
+        ctypes.c_float(svf), ctypes.c_float(mba), ssu, ssv, _p(o), nthreads or nthreads_default(),
+    )
+    if oob:
+        msg = f"reference projector read outside the volume {oob} times"
+        raise RuntimeError(msg)
+    return o
+
+
+def ref_backproject(
+    specs: np.ndarray,
+    projs: np.ndarray,
+    vol: np.ndarray,
+    cfg_contents: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    mult: np.ndarray | None = None,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """The reference's backproject_CB_voltex<float,float> on the CPU; accumulates into ``vol`` (C order float32)."""
+    lib = _load(REF_SO)
+    lib.ref_backproject.restype = ctypes.c_longlong
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    p = np.ascontiguousarray(projs, dtype=np.float32)
+    if not (vol.flags["C_CONTIGUOUS"] and vol.dtype == np.float32):
+        msg = "vol must be a C-contiguous float32 array"
+        raise ValueError(msg)
+    mm = None if mult is None else np.ascontiguousarray(mult, dtype=np.float32)
+    c = cfg_contents
+    tp = np.asarray(corner, dtype=np.float32)
+    f = ctypes.c_float
+    oob = lib.ref_backproject(
+        _p(s), m, nu, nv, _p(p), _p(vol), vol.shape[0], vol.shape[1], vol.shape[2], f(voxwid), _p(tp),
+        None if mm is None else _p(mm), int(c["exact"]), int(c["backproject_all_1s"]), int(c["mask_to_cylinder"]),
+        f(float(c["mask_to_cyl_rad"])), f(float(c["soften_edge_proportion"])), int(c["Z_on_L_factor_power"]),
+        int(c["Z_on_val_factor_power"]), f(float(c["Z_on_val_factor_val"])), int(c["approx_mode_direct_raycast"]),
+        int(c["approx_mode_linear_interpolate"]), int(c["ssx"]), int(c["ssy"]), int(c["ssz"]),
+        nthreads or nthreads_default(),
+    )
+    if oob:
+        msg = f"reference backprojector accessed outside the volume {oob} times"
+        raise RuntimeError(msg)
+    return vol
