@@ -8,9 +8,9 @@ Landweber_flatpanel). Kernels live in libaprict_b200.so, reached through the C
 ABI in include/aprict_b200.h.
 """
 
-from . import cb
-from .volume import FBVolume, Volume
+from .volume import FBVolume, Volume  # noqa: I001  (iterators import Volume from here)
+from . import cb, iterators
 
 __version__ = "0.1.0"
 
-__all__ = ["FBVolume", "Volume", "__version__", "cb"]
+__all__ = ["FBVolume", "Volume", "__version__", "cb", "iterators"]

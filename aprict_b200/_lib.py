@@ -45,6 +45,13 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         _c_int,
         [_c_void_p, _c_void_p, ctypes.c_float, _c_void_p, ctypes.c_int64, _c_void_p],
     ),
+    "aprict_b200_ramp_filter": (
+        _c_int,
+        [
+            _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_int, _c_void_p,
+            ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
+        ],
+    ),
 }
 
 _lock = threading.Lock()

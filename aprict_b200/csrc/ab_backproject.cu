@@ -30,6 +30,7 @@ struct BPParams {
     const aprict_proj_spec *specs;
     uint32_t n_views, nu, nv;
     ab_pstrides ps;
+    int su, sv;  // u, v element strides (32-bit: in-view offsets are checked to fit)
     const float *projs;
     float *vol;
     const float *mult;
@@ -41,7 +42,7 @@ struct BPParams {
     int mask;
     float mask_r2;
     int all_ones;
-    float sep;
+    float sep, inv_sep;
     int pL, pV;
     float val;
     int ssx, ssy, ssz;
@@ -59,30 +60,31 @@ __device__ __forceinline__ bool near_half(float f) {
     return fabsf(g - rintf(g)) < kRefine;
 }
 
-__device__ __forceinline__ float fetch_nearest(const BPParams &P, int view, float fu, float fv, const float xw[3]) {
+// pv: this view's image; in-view offsets fit in 32 bits (checked on the host).
+__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pv, int view, float fu, float fv,
+                                               float x, float y, float z) {
     if (near_half(fu) || near_half(fv)) {
         double du, dv;
         const aprict_proj_spec sp = P.specs[view];
-        ab_project_point_d(sp, ab_d3{(double)xw[0], (double)xw[1], (double)xw[2]}, du, dv);
+        ab_project_point_d(sp, ab_d3{(double)x, (double)y, (double)z}, du, dv);
         const int iu = (int)floor(du + 0.5), iv = (int)floor(dv + 0.5);
         if (iu < 0 || iu >= (int)P.nu || iv < 0 || iv >= (int)P.nv) return 0.f;
-        return __ldg(P.projs + (int64_t)view * P.ps.view + (int64_t)iu * P.ps.u + (int64_t)iv * P.ps.v);
+        return __ldg(pv + (iu * P.su + iv * P.sv));
     }
     const float gu = floorf(fu + 0.5f), gv = floorf(fv + 0.5f);
     if (!(gu >= 0.f && gu < (float)P.nu && gv >= 0.f && gv < (float)P.nv)) return 0.f;
-    return __ldg(P.projs + (int64_t)view * P.ps.view + (int64_t)gu * P.ps.u + (int64_t)gv * P.ps.v);
+    return __ldg(pv + ((int)gu * P.su + (int)gv * P.sv));
 }
 
 // Bilinear rule of get_bilinear_interp (CB_backproject.cu:221-254), same
 // operation order.
-__device__ __forceinline__ float fetch_bilinear(const BPParams &P, int view, float fu, float fv) {
+__device__ __forceinline__ float fetch_bilinear(const BPParams &P, const float *pv, float fu, float fv) {
     if (fu <= -1.f || fv <= -1.f || fu >= (float)P.nu || fv >= (float)P.nv) return 0.f;
     const int i0 = (int)floorf(fu), j0 = (int)floorf(fv);
     const float fx = fu - (float)i0, fy = fv - (float)j0;
-    const float *base = P.projs + (int64_t)view * P.ps.view;
     auto get = [&](int i, int j) -> float {
         if (i < 0 || i >= (int)P.nu || j < 0 || j >= (int)P.nv) return 0.f;
-        return __ldg(base + (int64_t)i * P.ps.u + (int64_t)j * P.ps.v);
+        return __ldg(pv + (i * P.su + j * P.sv));
     };
     const float v00 = get(i0, j0), v01 = get(i0, j0 + 1), v10 = get(i0 + 1, j0), v11 = get(i0 + 1, j0 + 1);
     const float t1 = v00 * (1.f - fx) + v10 * fx;
@@ -174,6 +176,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                     for (int t = 0; t < cn; ++t) {
                         const int view = (int)v0 + t;
                         const ab_bpview b = sv[t];
+                        const float *pvw = P.projs + (int64_t)view * P.ps.view;
                         const float Nu0 = dot4(b.nu, X0, Y0, Z0), Nv0 = dot4(b.nv, X0, Y0, Z0);
                         const float D0 = dot4(b.den, X0, Y0, Z0);
                         const float dNu = (a2 == 0 ? b.nu.x : (a2 == 1 ? b.nu.y : b.nu.z)) * vw;
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                             if (!live[k]) continue;
                             const float kf = (float)k;
                             const float D = fmaf(kf, dD, D0);
-                            const float rD = 1.f / D;
+                            const float rD = __frcp_rn(D);
                             const float fu = fmaf(kf, dNu, Nu0) * rD;
                             const float fv = fmaf(kf, dNv, Nv0) * rD;
                             float s;
@@ -224,7 +227,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                 float cx[3] = {X0, Y0, Z0};
                                 cx[a2] += kf * vw;
                                 const float r0x = e.s.x - cx[0], r0y = e.s.y - cx[1], r0z = e.s.z - cx[2];
-                                const float *pb = P.projs + (int64_t)view * P.ps.view;
                                 s = 0.f;
                                 for (int iu = ulo; iu <= uhi; ++iu) {
                                     const float dux = fmaf(e.u.x, (float)iu, e.d0.x);
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                         float a_lo = 0.f, a_hi = 3.0e38f;
                                         bool miss = false;
                                         if (dx != 0.f) {
-                                            const float inv = 1.f / dx;
+                                            const float inv = __frcp_rn(dx);
                                             const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                             miss |= fabsf(r0x) > h;
                                         }
                                         if (dy != 0.f) {
-                                            const float inv = 1.f / dy;
+                                            const float inv = __frcp_rn(dy);
                                             const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                             miss |= fabsf(r0y) > h;
                                         }
                                         if (dz != 0.f) {
-                                            const float inv = 1.f / dz;
+                                            const float inv = __frcp_rn(dz);
                                             const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -262,9 +264,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                         }
                                         if (miss || !(a_hi > a_lo)) continue;
                                         const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
-                                        const float pv =
-                                            P.all_ones ? 1.f
-                                                       : __ldg(pb + (int64_t)iu * P.ps.u + (int64_t)iv * P.ps.v);
+                                        const float pv = P.all_ones ? 1.f : __ldg(pvw + (iu * P.su + iv * P.sv));
                                         s = fmaf(pv, chord, s);
                                     }
                                 }
@@ -294,18 +294,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                 float pv = 0.f;
                                 if (w != 0.f) {
                                     if (BILIN) {
-                                        pv = fetch_bilinear(P, view, fu, fv);
+                                        pv = fetch_bilinear(P, pvw, fu, fv);
                                     } else {
                                         float xw[3] = {X0 + P.c0[0], Y0 + P.c0[1], Z0 + P.c0[2]};
                                         xw[a2] += kf * vw;
-                                        pv = fetch_nearest(P, view, fu, fv, xw);
+                                        pv = fetch_nearest(P, pvw, view, fu, fv, xw[0], xw[1], xw[2]);
                                     }
                                 }
                                 s = pv * w;
                             }
                             if (P.sep > 0.f && s != 0.f) {
-                                s *= ab_edge_taper(fu - (b.halfu - 0.5f), fv - (b.halfv - 0.5f), b.halfu, b.halfv,
-                                                   P.sep);
+                                s *= ab_edge_taper(fu - (b.halfu - 0.5f), fv - (b.halfv - 0.5f), b.inv_halfu, b.inv_halfv,
+                                                   P.inv_sep);
                             }
                             acc[k] += s;
                         }
@@ -385,6 +385,10 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.nv = pd->nv;
     P.ps = ab_pstrides{pd->stride_view, pd->stride_u, pd->stride_v};
     P.projs = projs_dev;
+    P.su = (int)pd->stride_u;
+    P.sv = (int)pd->stride_v;
+    if ((int64_t)(pd->nu - 1) * pd->stride_u + (int64_t)(pd->nv - 1) * pd->stride_v + 1 > 0x7fffffffLL)
+        return ab_fail(APRICT_ERR_TOO_LARGE, "one projection image spans more than 2^31 elements");
     P.vol = vol_dev;
     P.mult = multiplier_dev;
     P.n[0] = (int)vd->nx;
@@ -407,6 +411,7 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.mask_r2 = cfg->mask_to_cyl_rad * cfg->mask_to_cyl_rad;
     P.all_ones = cfg->backproject_all_1s ? 1 : 0;
     P.sep = cfg->soften_edge_proportion;
+    P.inv_sep = P.sep > 0.f ? 1.f / P.sep : 0.f;
     P.pL = cfg->Z_on_L_factor_power;
     P.pV = cfg->Z_on_val_factor_power;
     P.val = cfg->Z_on_val_factor_val;

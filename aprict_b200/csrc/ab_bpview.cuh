@@ -29,6 +29,7 @@ struct ab_bpview {
     float invL;  // 1 / |L|
     float halfu; // nu / 2
     float halfv; // nv / 2
+    float inv_halfu, inv_halfv;
 };
 
 // Exact-mode extras: ray origin and per-pixel direction in world units,
@@ -69,6 +70,8 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     o.invL = (float)(1.0 / Lnorm);
     o.halfu = (float)sp.nu * 0.5f;
     o.halfv = (float)sp.nv * 0.5f;
+    o.inv_halfu = (float)(2.0 / (double)sp.nu);
+    o.inv_halfv = (float)(2.0 / (double)sp.nv);
     return true;
 }
 
@@ -109,13 +112,15 @@ AB_HD float ab_powint(float b, int e) {
 }
 
 // Detector-edge cosine taper (CB_backproject.cu:694-713); cu, cv are
-// coordinates relative to the detector centre in pixels.
-AB_HD float ab_edge_taper(float cu, float cv, float halfu, float halfv, float sep) {
-    float ud = fabsf(cu) / halfu;
-    float vd = fabsf(cv) / halfv;
-    ud = fmaxf(0.f, fminf(1.f, (1.f - ud) / sep));
-    vd = fmaxf(0.f, fminf(1.f, (1.f - vd) / sep));
-    // (1 + cos(pi (1 - x))) / 2 == (1 - cos(pi x)) / 2
+// coordinates relative to the detector centre in pixels. Outside the edge
+// band the clamped argument is 1 and the factor is exactly 1, so the cosines
+// are only evaluated inside the band.
+AB_HD float ab_edge_taper(float cu, float cv, float inv_halfu, float inv_halfv, float inv_sep) {
+    float ud = fabsf(cu) * inv_halfu;
+    float vd = fabsf(cv) * inv_halfv;
+    ud = fmaxf(0.f, fminf(1.f, (1.f - ud) * inv_sep));
+    vd = fmaxf(0.f, fminf(1.f, (1.f - vd) * inv_sep));
+    if (ud == 1.f && vd == 1.f) return 1.f;
     ud = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - ud))) * 0.5f));
     vd = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - vd))) * 0.5f));
     return ud * vd;

@@ -162,31 +162,28 @@ AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visi
     float kx = 0.f, ky = 0.f, kz = 0.f;
     float tx = t0x, ty = t0y, tz = t0z;
     float t = 0.f;
+    // Branch-free step: every lane of a warp runs the same instructions
+    // whichever axis its ray crosses next (a 3-way branch would serialise).
     for (;;) {
         const float tm = fminf(tx, fminf(ty, tz));
         const float te = fminf(tm, tend);
         visit(te - t, off);
         if (tm >= tend) break;
         t = tm;
-        if (tx == tm) {
-            ix += sx;
-            if (ix == lx) break;
-            off += ox;
-            kx += 1.f;
-            tx = fmaf(kx, dtx, t0x);
-        } else if (ty == tm) {
-            iy += sy;
-            if (iy == ly) break;
-            off += oy;
-            ky += 1.f;
-            ty = fmaf(ky, dty, t0y);
-        } else {
-            iz += sz;
-            if (iz == lz) break;
-            off += oz;
-            kz += 1.f;
-            tz = fmaf(kz, dtz, t0z);
-        }
+        const bool bx = tx == tm;
+        const bool by = !bx && (ty == tm);
+        const bool bz = !bx && !by;
+        off += bx ? ox : (by ? oy : oz);
+        ix += bx ? sx : 0;
+        iy += by ? sy : 0;
+        iz += bz ? sz : 0;
+        if ((ix == lx) | (iy == ly) | (iz == lz)) break;
+        kx += bx ? 1.f : 0.f;
+        ky += by ? 1.f : 0.f;
+        kz += bz ? 1.f : 0.f;
+        tx = bx ? fmaf(kx, dtx, t0x) : tx;
+        ty = by ? fmaf(ky, dty, t0y) : ty;
+        tz = bz ? fmaf(kz, dtz, t0z) : tz;
     }
     return true;
 }

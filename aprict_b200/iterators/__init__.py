@@ -1,0 +1,6 @@
+"""Iterative reconstruction (drop-in for ``aprict.iterators``)."""
+
+from .landweber_vram import Landweber_flatpanel
+from .sirt_vram import SIRT_flatpanel
+
+__all__ = ["Landweber_flatpanel", "SIRT_flatpanel"]

@@ -1,0 +1,82 @@
+"""Analytic reconstruction drivers.
+
+``fbp_fan_circ`` is the fan-beam FBP of the reference's ``aprict recon
+fbp-fan-circ`` (src/aprict/scripts/cli.py:85-96 -> recon_cbfp_cyl_fbp.py with
+fan_beam=True): per projection, weight by 1/sqrt(1 + u^2) and ramp-filter
+with Ram-Lak taps at pitch pixwid/L (FBPFilterer, ramp_filter.py:343-449),
+then backproject with direct-raycast weight (Z/R)^-2 (recon_cbfp_cyl_fbp.py:1108-1121;
+CB_backproject.cu:512-528) inside the reconstructable cylinder, and scale by
+1/(4 pi R M) (recon_cbfp_cyl_fbp.py:551-557).
+
+Here the whole stack is filtered in one kernel launch with the weights and the
+final scale folded in, then backprojected in one launch (the reference loops
+over chunks of projections with several array passes each).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .cb import flatpanel as fp
+from .cb.ramp_filter import FBPFilterer
+from .volume import Volume
+
+
+def fan_geometry(pg: fp.ProjGeom) -> tuple[float, float, float, int, int]:
+    """(R, L, pixwid, nu, nv) of a circular scan, with the reference's checks (recon_cbfp_cyl_fbp.py:459-496)."""
+    if len(pg.projs_list_shape) != 1:
+        msg = f"Input projection geometry has a non-flat shape: {pg.projs_list_shape}."
+        raise NotImplementedError(msg)
+    nus, nvs = np.broadcast_to(pg.nu, pg.projs_list_shape), np.broadcast_to(pg.nv, pg.projs_list_shape)
+    if not (np.all(nus == nus[0]) and np.all(nvs == nvs[0])):
+        msg = "Inconsistent detector resolution."
+        raise NotImplementedError(msg)
+    pixwids = np.linalg.norm(np.broadcast_to(pg.det_uvec, pg.projs_list_shape + (3,)), axis=-1)
+    pixheis = np.linalg.norm(np.broadcast_to(pg.det_vvec, pg.projs_list_shape + (3,)), axis=-1)
+    if not (np.allclose(pixwids, pixwids[0]) and np.allclose(pixheis, pixheis[0]) and np.isclose(pixwids[0], pixheis[0])):
+        msg = "Inconsistent or non-square detector pixels."
+        raise NotImplementedError(msg)
+    src = np.broadcast_to(pg.source_pos, pg.projs_list_shape + (3,)).astype(np.float64)
+    det = np.broadcast_to(pg.det_pos, pg.projs_list_shape + (3,)).astype(np.float64)
+    Rs = np.hypot(src[:, 0], src[:, 1])  # noqa: N806
+    if not np.allclose(Rs, Rs[0]):
+        msg = "Inconsistent source radius."
+        raise NotImplementedError(msg)
+    Ls = Rs + np.hypot(det[:, 0], det[:, 1])  # noqa: N806
+    if not np.allclose(Ls, Ls[0]):
+        msg = "Inconsistent source-to-detector length."
+        raise NotImplementedError(msg)
+    return float(Rs[0]), float(Ls[0]), float(pixwids[0]), int(nus[0]), int(nvs[0])
+
+
+def fbp_fan_circ(
+    projs: fp.ProjectionSet,
+    volume: Volume,
+    *,
+    interpolate: bool = False,
+    apodization: str | None = None,
+    cyl_mask_rad: float | None = None,
+    filtered_out: torch.Tensor | None = None,
+) -> Volume:
+    """Add the fan-beam FBP reconstruction of ``projs`` (M, nu, 1) into ``volume``."""
+    if projs.data is None:
+        msg = "You must provide projection data."
+        raise ValueError(msg)
+    R, L, pixwid, nu, nv = fan_geometry(projs.proj_geom)  # noqa: N806
+    m = projs.proj_geom.num_projs
+    filt = FBPFilterer(L=L, physpixwid=pixwid, proj_2d_shape=(nu, nv), _hacky_fan_beam_mode=True, apodization=apodization)
+    scale = 1.0 / (4.0 * np.pi * R * m)
+    outs = None if filtered_out is None else [filtered_out]
+    (filtered,) = filt.rfilt.filter(projs.data, weights=filt._weights, scale=scale, outs=outs)  # noqa: SLF001
+    support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
+    cfg = fp.ConfigBackproject(
+        fast_approx=True,
+        cyl_mask_rad=cyl_mask_rad or support,
+        Z_on_val_factor_power=-2,
+        Z_on_val_factor_val=R,
+        approx_mode_direct_raycast=True,
+        approx_mode_bilinear_interpolate=interpolate,
+    )
+    fp.backproject(cfg, volume, fp.ProjectionSet(projs.proj_geom, data=filtered))
+    return volume

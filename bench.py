@@ -1,0 +1,495 @@
+"""Benchmark: SIRT iterations/s (with forward rays/s and back voxel-updates/s) on one B200.
+
+Workload (default ``sirt256``): a 256^3 float32 volume (0.5 mm voxels) of 30
+seeded random ellipsoids, a circular cone-beam scan of 360 views on a 384x384
+flat detector (0.8 mm pixels, SOD 500 mm, SDD 1000 mm), and the reference's
+SIRT iteration x <- x + M (.) B (b - A x) (src/aprict/iterators/sirt_vram.py:130-152):
+A the exact Siddon projector, B the fast backprojector with cylinder mask and
+5 % detector-edge taper, M the preconditioner. The data b are synthetic
+(A x_true + Poisson noise at 1e5 photons); nothing is read from disk.
+
+A step is one SIRT iteration. ``value`` is the batched form (fused residual +
+one all-view backprojection, replayed from a captured CUDA graph); the
+plain-launch form of the same kernels (copy, atomic projection, 10-view
+backprojection launches with host synchronisation -- the reference's launch
+pattern) is reported beside it. The inputs (b 202 MB, residual 202 MB, x and
+M 64 MB each) exceed the 126 MB L2, so no flush is needed between steps.
+
+``--impl reference`` times the reference's own device code compiled for the CPU
+(oracle/_ref), on a bounded sample of the same iteration scaled to iter/s.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SIRT iter/s"
+BASELINE_METRIC = "fwd rays/s, back voxel-updates/s, SIRT iter/s: batched vs plain at rel L2 1e-5"
+
+WORKLOADS = {
+    "sirt256": dict(
+        n=256, voxwid=0.5, n_ellipsoids=30, views=360, det=384, pix_at_iso=0.4, R=500.0, LmR=500.0, photons=1e5,
+        seed=4,
+    ),
+    "small": dict(n=96, voxwid=1.0, n_ellipsoids=10, views=90, det=128, pix_at_iso=0.8, R=300.0, LmR=300.0, photons=1e5, seed=1),
+}
+
+
+def _env_rank() -> tuple[int, int, int]:
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_problem(w: dict):
+    from aprict_b200 import phantoms
+    from aprict_b200.cb import flatpanel as fp
+
+    n = w["n"]
+    pg = fp.ProjGeom.new_circular_scan(
+        num_source_points=w["views"], R=w["R"], L_minus_R=w["LmR"], pix_widhei_at_isocenter=(w["pix_at_iso"],) * 2,
+        num_pix_widhei=(w["det"], w["det"]),
+    )
+    x_true = phantoms.ellipsoid_volume(w["seed"], w["n_ellipsoids"], (n, n, n), w["voxwid"], semi_axes_vox=(10, 80 * n / 256))
+    return pg, x_true
+
+
+def simulate_data(pg, x_true: np.ndarray, w: dict):
+    """b = -log(Poisson(I0 exp(-A x))/I0), capped at log I0 (examples/fan_beam_sirt.py:156-180)."""
+    import torch
+
+    from aprict_b200 import Volume
+    from aprict_b200.cb import flatpanel as fp
+
+    v = Volume(x_true, voxwid=w["voxwid"])
+    ps = fp.ProjectionSet(pg, data=None)
+    fp.project(fp.ConfigProject(), v, ps, block=True)
+    g = torch.Generator(device="cuda").manual_seed(w["seed"])
+    lam = w["photons"] * torch.exp(-ps.data.double())
+    counts = torch.poisson(lam, generator=g).clamp_(min=1.0)
+    b = (-torch.log(counts / w["photons"])).clamp_(max=float(np.log(w["photons"]))).float()
+    return b
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = pathlib.Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")  # noqa: SIM115
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.fh, stderr=subprocess.DEVNULL,
+            )
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict | None:
+        if self.proc is None or not self.path.exists():
+            return None
+        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, val in zip(names, r[5:9]):
+                if "Active" in val and "Not" not in val:
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(rows),
+        }
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic() -> dict:
+    p = ROOT / "profiles" / "traffic.json"
+    return json.loads(p.read_text()) if p.exists() else {}
+
+
+def count_segments(pg, x_shape, voxwid: float, sample_views: int = 4) -> tuple[float, int]:
+    """Sum of ray/voxel segments over the whole scan, from the FP64 oracle on a view sample.
+
+    Circular scans are rotationally equivalent up to the volume's cubic
+    symmetry, so the per-view count of evenly spaced sample views scales.
+    """
+    from oracle import oracle
+
+    m = pg.num_projs
+    idx = list(np.linspace(0, m, sample_views, endpoint=False).astype(int))
+    specs = pg.to_proj_spec_array()[idx]
+    ones = np.ones(x_shape, np.float32)
+    corner = -np.float32(voxwid) * np.array(x_shape, np.float32) / 2
+    _, nseg = oracle.project_siddon(specs, ones, voxwid=voxwid, corner=corner)
+    return nseg * m / sample_views, nseg
+
+
+def run_ours(args) -> dict:
+    import torch
+    import torch.distributed as dist
+
+    from aprict_b200 import Volume
+    from aprict_b200.cb import flatpanel as fp
+    from aprict_b200.iterators import SIRT_flatpanel
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    w = WORKLOADS[args.workload]
+    n = w["n"]
+    pg, x_true = make_problem(w)
+    b = simulate_data(pg, x_true, w)
+    meas = fp.ProjectionSet(pg, data=b)
+    x = Volume.zeros((n, n, n), voxwid=w["voxwid"])
+    sirt = SIRT_flatpanel(SIRT_flatpanel.Config(), x, meas)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+
+    def barrier() -> None:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- component kernels (CUDA events on the launching stream) ----
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    def time_op(fn, reps: int) -> float:
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        s, e = ev(), ev()
+        s.record(stream)
+        for _ in range(reps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    cfg_res = fp.ConfigProject(multiply_before_adding=-1)
+    r = sirt._scratch  # noqa: SLF001
+    t_fp = time_op(lambda: fp.project_residual(cfg_res, x, r, meas.data), 3)
+    t_bp = time_op(lambda: fp.backproject(sirt._config_bp, x, r, summand_multiplier=sirt.preconditioner), 3)  # noqa: SLF001
+    x.fill(0.0)
+
+    # ---- batched: graph-captured iterations ----
+    sirt.iterate_graph(1)  # warm-up + capture (1 iteration per replay)
+    sirt.iterate_graph(1)
+    for _ in range(max(0, args.warmup - 2)):
+        sirt.iterate_graph(1)
+    barrier()
+    with ClockSampler(local) as clk:
+        s, e = ev(), ev()
+        s.record(stream)
+        for _ in range(args.steps):
+            sirt.iterate_graph(1)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / args.steps
+    ms = max_over_ranks(ms)
+    barrier()
+
+    # ---- plain launches: the reference's pattern with the same kernels ----
+    chunks = []
+    for c0 in range(0, pg.num_projs, 10):
+        sl = slice(c0, min(c0 + 10, pg.num_projs))
+        chunks.append(fp.ProjectionSet(pg.sliced(sl), data=r.data[sl]))
+    cfg_acc = fp.ConfigProject(multiply_before_adding=-1)
+
+    def plain_iter() -> None:
+        r.data.copy_(meas.data)
+        fp.project(cfg_acc, x, r, block=True)
+        for ch in chunks:
+            fp.backproject(sirt._config_bp, x, ch, summand_multiplier=sirt.preconditioner)  # noqa: SLF001
+        torch.cuda.synchronize()
+
+    for _ in range(2):
+        plain_iter()
+    barrier()
+    t0 = time.perf_counter()
+    s, e = ev(), ev()
+    s.record(stream)
+    k_plain = max(3, args.steps // 2)
+    for _ in range(k_plain):
+        plain_iter()
+    e.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = max_over_ranks(s.elapsed_time(e) / k_plain)
+
+    # ---- end to end through the public API with host buffers ----
+    b_host = b.cpu().pin_memory()
+    x_host = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
+    def e2e_iter() -> None:
+        meas.data.copy_(b_host, non_blocking=True)
+        sirt.iterate()
+        x_host.copy_(x.data, non_blocking=True)
+
+    for _ in range(2):
+        e2e_iter()
+    barrier()
+    s, e = ev(), ev()
+    s.record(stream)
+    for _ in range(args.steps):
+        e2e_iter()
+    e.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = max_over_ranks(s.elapsed_time(e) / args.steps)
+
+    # ---- accounting ----
+    M = pg.num_projs
+    rays = M * w["det"] ** 2
+    vox = n**3
+    nseg, nseg_sample = count_segments(pg, (n, n, n), w["voxwid"])
+    fp_bytes = 4.0 * nseg + 8.0 * rays  # one gather per segment; read b, write r
+    bp_bytes = 4.0 * vox * M + 12.0 * vox  # one detector sample per voxel-view; read M, RMW x
+    peak, peak_kind = load_peaks()
+    fp_gbs = fp_bytes / (t_fp * 1e-3) / 1e9
+    bp_gbs = bp_bytes / (t_bp * 1e-3) / 1e9
+    dom = "project_siddon" if t_fp >= t_bp else "backproject"
+    traffic = load_traffic().get(f"{dom}:{args.workload}")
+    roof = {
+        "bound": "hbm",
+        "kernel": dom,
+        "achieved": round(fp_gbs if dom == "project_siddon" else bp_gbs, 1),
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": round((fp_gbs if dom == "project_siddon" else bp_gbs) / peak, 4),
+        "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+        "traffic": traffic,
+        "model": "FP: 4 B per ray/voxel segment + 8 B per ray; BP: 4 B per voxel-view + 12 B per voxel",
+    }
+    out = {
+        "metric": METRIC,
+        "value": round(world * 1000.0 / ms, 4),
+        "unit": "iter/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid phantom, simulated Poisson data)",
+        "config": {
+            "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector, SOD {w['R']} SDD {w['R'] + w['LmR']}",
+            "baseline_metric": BASELINE_METRIC,
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "l2": "inputs larger than L2 (b+r 404 MB, x+M 128 MB)",
+            "form": "batched: fused residual + all-view backprojection, CUDA-graph replay",
+        },
+        "components": {
+            "fwd_rays_per_s": round(rays / (t_fp * 1e-3), 1),
+            "fwd_ray_steps_per_s": round(nseg / (t_fp * 1e-3), 1),
+            "back_voxel_updates_per_s": round(vox * M / (t_bp * 1e-3), 1),
+            "fp_ms": round(t_fp, 4),
+            "bp_ms": round(t_bp, 4),
+            "fp_GBps": round(fp_gbs, 1),
+            "bp_GBps": round(bp_gbs, 1),
+            "segments_per_scan": nseg,
+            "plain_iter_per_s": round(world * 1000.0 / ms_plain, 4),
+            "plain_ms_per_step": round(ms_plain, 4),
+            "batched_over_plain": round(ms_plain / ms, 3),
+        },
+        "roofline": roof,
+        "e2e": {
+            "value": round(world * 1000.0 / ms_e2e, 4),
+            "unit": "iter/s",
+            "h2d_bytes_per_step": int(b.numel() * 4),
+            "d2h_bytes_per_step": int(x.data.numel() * 4),
+            "api": "SIRT_flatpanel.iterate() with b copied from pinned host memory and x read back each step",
+        },
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_reference(pg, x_true, w, b.cpu().numpy(), sirt)
+    if world > 1:
+        dist.destroy_process_group()
+    return out if rank == 0 else {}
+
+
+def cpu_reference(pg, x_true: np.ndarray, w: dict, b: np.ndarray, sirt=None) -> dict:
+    """Time one SIRT iteration of the reference's own kernels compiled for the CPU, on a view sample."""
+    from aprict_b200.cb import flatpanel as fp
+    from oracle import oracle
+
+    kind = "reference" if oracle.have_ref() else "port"
+    n = w["n"]
+    M = pg.num_projs
+    specs = pg.to_proj_spec_array()
+    corner = -np.float32(w["voxwid"]) * np.array((n, n, n), np.float32) / 2
+    threads = os.cpu_count() or 1
+    fp_views = max(1, min(M, int(os.environ.get("APRICT_CPU_FP_VIEWS", "12"))))
+    bp_views = max(1, min(M, int(os.environ.get("APRICT_CPU_BP_VIEWS", "10"))))
+    x0 = x_true.astype(np.float32)
+    sel = np.linspace(0, M, fp_views, endpoint=False).astype(int)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        oracle.ref_project_siddon(specs[sel], x0, voxwid=w["voxwid"], corner=corner, mba=-1.0)
+    else:
+        oracle.project_siddon(specs[sel], x0, voxwid=w["voxwid"], corner=corner, mba=-1.0)
+    t_fp = (time.perf_counter() - t0) * M / fp_views
+    cfg = fp.ConfigBackproject(
+        fast_approx=True, cyl_mask_rad=n / 2 * w["voxwid"], apply_summand_multiplier=True, soften_det_edges_proportion=0.05
+    )
+    mult = np.ones((n, n, n), np.float32)
+    vol = np.zeros((n, n, n), np.float32)
+    selb = np.linspace(0, M, bp_views, endpoint=False).astype(int)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        oracle.ref_backproject(specs[selb], b[selb], vol, cfg.contents, voxwid=w["voxwid"], corner=corner, mult=mult)
+    else:
+        oracle.backproject(specs[selb], b[selb], (n, n, n), cfg.contents, voxwid=w["voxwid"], corner=corner, mult=mult)
+    t_bp = (time.perf_counter() - t0) * M / bp_views
+    t_iter = t_fp + t_bp
+    return {
+        "value": round(1.0 / t_iter, 6),
+        "unit": "iter/s",
+        "cores": threads,
+        "kind": kind,
+        "sample": f"projection of {fp_views}/{M} views and backprojection of {bp_views}/{M} views, scaled to the full iteration ({t_fp:.1f} s + {t_bp:.1f} s per iteration)",
+    }
+
+
+def run_reference(args) -> dict:
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return {}
+    w = WORKLOADS[args.workload]
+    pg, x_true = make_problem(w)
+    n = w["n"]
+    # b from the oracle's own projection of the phantom (no GPU on this arm)
+    from oracle import oracle
+
+    M = pg.num_projs
+    b = np.zeros((M, w["det"], w["det"]), np.float32)
+    vals = []
+    for _ in range(args.warmup):
+        cpu_reference(pg, x_true, w, b)
+    for _ in range(args.steps):
+        vals.append(cpu_reference(pg, x_true, w, b))
+    v = statistics.median(c["value"] for c in vals)
+    base = vals[0]
+    base["value"] = v
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "iter/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1000.0 / v, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid phantom)",
+        "config": {
+            "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector",
+            "baseline_metric": BASELINE_METRIC,
+            "where": "reference device code compiled for the host CPU (oracle/_ref), OpenMP over rays/voxels",
+            "oracle_kind": "reference" if oracle.have_ref() else "port",
+        },
+        "cpu_baseline": base,
+        "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def profile_kernels(args) -> dict:
+    """Launch the workload's kernels a few times and exit (a small driver for ncu captures).
+
+    Launch order: 1 projection (simulated data), then ``--steps`` x (fused
+    residual projection, all-view backprojection); nothing else runs on the GPU.
+    """
+    import torch
+
+    from aprict_b200 import Volume
+    from aprict_b200.cb import flatpanel as fp
+
+    w = WORKLOADS[args.workload]
+    n = w["n"]
+    pg, x_true = make_problem(w)
+    b = simulate_data(pg, x_true, w)
+    meas = fp.ProjectionSet(pg, data=b)
+    x = Volume(x_true * 0.5, voxwid=w["voxwid"])
+    M = Volume(np.full((n, n, n), 1e-3, np.float32), voxwid=w["voxwid"])  # noqa: N806
+    r = meas.zeroed_copy()
+    cfg_bp = fp.ConfigBackproject(
+        fast_approx=True, cyl_mask_rad=n / 2 * w["voxwid"], apply_summand_multiplier=True, soften_det_edges_proportion=0.05
+    )
+    for _ in range(args.steps):
+        fp.project_residual(fp.ConfigProject(multiply_before_adding=-1), x, r, meas.data)
+        fp.backproject(cfg_bp, x, r, summand_multiplier=M)
+    torch.cuda.synchronize()
+    return {"mode": "kernels", "workload": args.workload, "launches": 1 + 2 * args.steps}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sirt256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.mode == "kernels":
+        out = profile_kernels(args)
+    else:
+        out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

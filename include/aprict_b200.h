@@ -208,6 +208,22 @@ APRICT_API int aprict_b200_vol_mul(float *out_dev, const float *a_dev, const flo
 APRICT_API int aprict_b200_vol_axpy(float *out_dev, const float *a_dev, float alpha, const float *b_dev,
                                     int64_t n, aprict_stream_t stream);
 
+/* ---- Ramp filtering ----
+ * out[view][m][v] = scale * sum_j taps[m - j + nu - 1] * w[j][v] * in[view][j][v]
+ * for m, j in [0, nu): the linear convolution the reference evaluates by
+ * zero-padded cuFFT (RampFilterer._filter_chunk_axis1, ramp_filter.py:139-240)
+ * after the cosine weighting of FBPFilterer (ramp_filter.py:407-449, :685-689).
+ *   taps_dev      : 2*nu-1 floats, h[-(nu-1)] .. h[nu-1]
+ *   odd_taps_only : nonzero if taps at even nonzero offsets are all zero (pure
+ *                   Ram-Lak); halves the work
+ *   weights_dev   : (nu, nv) per-pixel weights with element strides
+ *                   (w_stride_u, w_stride_v), or NULL for none
+ * in and out must not alias; nu <= 4096. */
+APRICT_API int aprict_b200_ramp_filter(const aprict_proj_desc *in, const float *in_dev,
+                                       const aprict_proj_desc *out, float *out_dev, const float *taps_dev,
+                                       int odd_taps_only, const float *weights_dev, int64_t w_stride_u,
+                                       int64_t w_stride_v, float scale, aprict_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

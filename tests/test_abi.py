@@ -1,0 +1,129 @@
+"""The C-ABI library loads, exports every declared symbol, and validates on the host.
+
+No compute call is made here: every call below fails argument validation
+before anything is launched, so these run without a GPU.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import re
+
+import numpy as np
+import pytest
+
+from aprict_b200 import _lib
+from aprict_b200 import _structs as S
+
+HEADER = pathlib.Path(__file__).resolve().parents[1] / "include" / "aprict_b200.h"
+
+
+def declared_symbols() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"APRICT_API[^;(]*?\b(aprict_b200_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points() -> None:
+    syms = declared_symbols()
+    assert "aprict_b200_project_siddon" in syms
+    assert "aprict_b200_backproject" in syms
+    assert len(syms) >= 10
+
+
+def test_library_exports_every_declared_symbol() -> None:
+    lib = _lib.lib()
+    for name in declared_symbols():
+        assert hasattr(lib, name), f"{name} declared in include/aprict_b200.h but not exported"
+
+
+def test_binding_covers_every_declared_symbol() -> None:
+    assert set(declared_symbols()) <= set(_lib.SIGNATURES), set(declared_symbols()) - set(_lib.SIGNATURES)
+
+
+def test_struct_layouts_match_c() -> None:
+    lib = _lib.lib()
+    for name, dt in S.ABI_STRUCTS.items():
+        assert lib.aprict_b200_struct_size(name.encode()) == dt.itemsize, name
+    assert lib.aprict_b200_struct_size(b"no_such_struct") == 0
+
+
+def test_status_strings() -> None:
+    lib = _lib.lib()
+    assert lib.aprict_b200_status_string(0) == b"ok"
+    assert lib.aprict_b200_status_string(1) == b"invalid argument"
+    assert lib.aprict_b200_status_string(999) == b"unknown status"
+    assert lib.aprict_b200_version().decode().count(".") == 2
+
+
+def _fake(n: int = 1 << 20) -> int:
+    """A host address standing in for a device pointer; never dereferenced because validation fails first."""
+    return 0x10000000
+
+
+@pytest.mark.parametrize(
+    ("field", "value", "expect"),
+    [("ssu", 0, ValueError), ("ssv", 100, ValueError), ("multiply_before_adding", np.inf, ValueError)],
+)
+def test_project_rejects_bad_config(field: str, value: float, expect: type) -> None:
+    lib = _lib.lib()
+    cfg = np.array((1.0, 1.0, 1, 1), dtype=S.project_config)
+    cfg[field] = value
+    pd = _lib.proj_desc((2, 4, 4), (16, 4, 1))
+    vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
+    rc = lib.aprict_b200_project_siddon(_fake(), _lib.ptr(pd), _fake(), None, _lib.ptr(vd), _fake(), _lib.ptr(cfg), None, None)
+    with pytest.raises(expect):
+        _lib.check(rc, "project")
+
+
+def test_project_rejects_bad_volume() -> None:
+    lib = _lib.lib()
+    cfg = np.array((1.0, 1.0, 1, 1), dtype=S.project_config)
+    pd = _lib.proj_desc((2, 4, 4), (16, 4, 1))
+    for vd in (
+        _lib.vol_desc((0, 4, 4), "C", 1.0, np.zeros(3)),
+        _lib.vol_desc((4, 4, 4), "C", -1.0, np.zeros(3)),
+        _lib.vol_desc((4, 4, 4), "C", 1.0, np.array([np.nan, 0, 0])),
+    ):
+        rc = lib.aprict_b200_project_siddon(_fake(), _lib.ptr(pd), _fake(), None, _lib.ptr(vd), _fake(), _lib.ptr(cfg), None, None)
+        assert rc == 1
+    # unaligned volume pointer
+    vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
+    rc = lib.aprict_b200_project_siddon(_fake(), _lib.ptr(pd), _fake(), None, _lib.ptr(vd), _fake() + 2, _lib.ptr(cfg), None, None)
+    assert rc == 1
+    assert b"aligned" in lib.aprict_b200_last_error()
+
+
+def test_project_empty_is_a_no_op() -> None:
+    lib = _lib.lib()
+    cfg = np.array((1.0, 1.0, 1, 1), dtype=S.project_config)
+    vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
+    pd = _lib.proj_desc((0, 4, 4), (16, 4, 1))
+    assert lib.aprict_b200_project_siddon(None, _lib.ptr(pd), None, None, _lib.ptr(vd), _fake(), _lib.ptr(cfg), None, None) == 0
+
+
+def test_backproject_validation() -> None:
+    lib = _lib.lib()
+    from aprict_b200.cb import flatpanel as fp
+
+    pd = _lib.proj_desc((2, 4, 4), (16, 4, 1))
+    vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
+    # multiplier flag without a multiplier
+    cfg = fp.ConfigBackproject(apply_summand_multiplier=True).contents
+    rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
+    assert rc == 1
+    # weighting presets other than 0 are not implemented
+    cfg = fp.ConfigBackproject(backproj_weighting_preset=3).contents
+    rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
+    assert rc == 2
+    with pytest.raises(NotImplementedError):
+        _lib.check(rc, "backproject")
+
+
+def test_volops_validation() -> None:
+    lib = _lib.lib()
+    assert lib.aprict_b200_vol_fill(None, 0, ctypes.c_float(1.0), None) == 0
+    assert lib.aprict_b200_vol_fill(None, 10, ctypes.c_float(1.0), None) == 1
+    assert lib.aprict_b200_vol_fill(_fake(), -1, ctypes.c_float(1.0), None) == 1
+    vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
+    assert lib.aprict_b200_vol_softmask_cylinder(_fake(), _lib.ptr(vd), ctypes.c_float(1.5), None) == 1
