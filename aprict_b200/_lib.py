@@ -52,6 +52,14 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
             ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
         ],
     ),
+    "aprict_b200_forbild_compile": (_c_int, [_c_void_p, ctypes.c_int64, _c_void_p]),
+    "aprict_b200_project_forbild": (
+        _c_int,
+        [
+            _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_uint32,
+            ctypes.c_uint32, _c_int, _c_void_p, _c_void_p, _c_void_p,
+        ],
+    ),
 }
 
 _lock = threading.Lock()

@@ -69,6 +69,36 @@ backproject_config = np.dtype(
     ]
 )
 
+forbild_clip = np.dtype(
+    {"names": ["axis", "dotprod", "mode"], "formats": [fvec3, "<f4", "u1"], "offsets": [0, 12, 16], "itemsize": 20}
+)
+
+# Byte-identical to the reference's FORBILD_Shape (FORBILD_volumes.h:1395-1415).
+forbild_shape = np.dtype(
+    {
+        "names": ["type", "rho", "cas1", "cas2", "cas3", "x", "y", "z", "dx", "dy", "dz", "r", "r1", "r2", "l",
+                  "a_x", "a_y", "a_z", "axis"],
+        "formats": ["u1", "<f4", forbild_clip, forbild_clip, forbild_clip] + ["<f4"] * 10 + [fvec3] * 4,
+        "offsets": [0, 4, 8, 28, 48, 68, 72, 76, 80, 84, 88, 92, 96, 100, 104, 108, 120, 132, 144],
+        "itemsize": 156,
+    }
+)
+
+quadric = np.dtype(
+    [
+        ("kind", "<i4"),
+        ("n_clip", "<i4"),
+        ("rho", "<f8"),
+        ("c", "<f8", (3,)),
+        ("M", "<f8", (9,)),
+        ("h", "<f8"),
+        ("alpha", "<f8"),
+        ("beta", "<f8"),
+        ("clip", "<f8", (3, 4)),
+        ("bb_half", "<f8", (3,)),
+    ]
+)
+
 # name in the C library -> numpy dtype, checked against sizeof() in tests.
 ABI_STRUCTS = {
     "aprict_proj_spec": proj_spec,
@@ -76,4 +106,6 @@ ABI_STRUCTS = {
     "aprict_proj_desc": proj_desc,
     "aprict_project_config": project_config,
     "aprict_backproject_config": backproject_config,
+    "aprict_forbild_shape": forbild_shape,
+    "aprict_quadric": quadric,
 }

@@ -441,6 +441,7 @@ class ConfigProject:
         ssu: int | None = None,
         ssv: int | None = None,
         overlap_addition: bool = False,
+        additive_line_integral: bool = False,
     ) -> None:
         # `x or 1` as in the reference: None and 0 both mean 1.
         svf = shrink_volume_factor or 1
@@ -451,6 +452,9 @@ class ConfigProject:
         # FORBILD path: later shapes take priority unless overlap_addition
         # (flatpanel.py:917-926; the reference hard-codes False).
         self._overlap_addition = bool(overlap_addition)
+        # additive mode in length units (sum rho * chord) instead of the
+        # reference's parametric sum (sum rho * dt)
+        self.additive_line_integral = bool(additive_line_integral)
 
     @property
     def contents(self) -> np.ndarray:

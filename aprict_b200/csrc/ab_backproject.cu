@@ -14,7 +14,10 @@
 // Each thread carries XB voxels along the slowest axis (independent
 // accumulators for ILP). Per-view coefficients (ab_bpview) are derived once per
 // CTA into shared memory and read as uniform broadcasts; the volume is read and
-// written exactly once per call instead of once per 10 views.
+// written exactly once per call instead of once per 10 views. CTAs are issued
+// in brick order (all of the fastest axis x a compact block of the other two)
+// so that the CTAs resident at one time project onto a small part of each
+// view and the projection data they gather stays in L2.
 #include <cuda_runtime.h>
 
 #include "ab_bpview.cuh"
@@ -29,15 +32,21 @@ constexpr int kXB = 4;         // voxels per thread along the slowest axis
 struct BPParams {
     const aprict_proj_spec *specs;
     uint32_t n_views, nu, nv;
-    ab_pstrides ps;
-    int su, sv;  // u, v element strides (32-bit: in-view offsets are checked to fit)
+    int64_t stride_view;
+    int su, sv;  // u, v element strides (in-view offsets are checked to fit 32 bits)
     const float *projs;
     float *vol;
     const float *mult;
-    int n[3];          // volume shape (x, y, z)
-    int64_t vs[3];     // element strides (x, y, z)
+    int n[3];        // volume shape (x, y, z)
+    int64_t vs[3];   // element strides (x, y, z)
     float voxwid;
-    float c0[3];       // volume centre (world)
+    float c0[3];     // volume centre (world)
+    double cornerd[3];
+    double vwd;
+    // brick-ordered CTA remap
+    int gb[3];       // blocks along fastest, middle, slowest axis
+    int sb1, sb2;    // super-brick extent in blocks along middle, slowest axis
+    int nsb1;        // super-bricks along the middle axis
     // config
     int mask;
     float mask_r2;
@@ -51,40 +60,51 @@ struct BPParams {
 
 // Pixel value with the reference's zero-order rule (get_zero_interp,
 // CB_backproject.cu:256-271): index floor(f + 0.5). When f + 0.5 lies within
-// kRefine of an integer the FP32 estimate cannot be trusted to pick the same
-// pixel as an exact evaluation, so the index is recomputed in FP64.
+// kRefine of an integer the FP32 estimate (error ~1e-4 pixel) cannot be
+// trusted to pick the pixel an exact evaluation picks, so the choice is made
+// again in FP64 from the voxel's FP64 position.
 constexpr float kRefine = 2e-3f;
 
-__device__ __forceinline__ bool near_half(float f) {
-    const float g = f + 0.5f;
-    return fabsf(g - rintf(g)) < kRefine;
+struct VoxRef {
+    int ix, iy, iz;    // voxel indices
+    float fx, fy, fz;  // sub-voxel offsets in voxels (0 without supersampling)
+};
+
+// Out of line: only the rare near-tie path pays for its FP64 registers.
+__device__ __noinline__ float refine_nearest(const BPParams &P, const float *pvw, int view, VoxRef r) {
+    const ab_d3 x{P.cornerd[0] + ((double)r.ix + 0.5 + (double)r.fx) * P.vwd,
+                  P.cornerd[1] + ((double)r.iy + 0.5 + (double)r.fy) * P.vwd,
+                  P.cornerd[2] + ((double)r.iz + 0.5 + (double)r.fz) * P.vwd};
+    double du, dv;
+    const aprict_proj_spec sp = P.specs[view];
+    ab_project_point_d(sp, x, du, dv);
+    const double gu = floor(du + 0.5), gv = floor(dv + 0.5);
+    if (!(gu >= 0.0 && gu < (double)P.nu && gv >= 0.0 && gv < (double)P.nv)) return 0.f;
+    return __ldg(pvw + ((int)gu * P.su + (int)gv * P.sv));
 }
 
-// pv: this view's image; in-view offsets fit in 32 bits (checked on the host).
-__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pv, int view, float fu, float fv,
-                                               float x, float y, float z) {
-    if (near_half(fu) || near_half(fv)) {
-        double du, dv;
-        const aprict_proj_spec sp = P.specs[view];
-        ab_project_point_d(sp, ab_d3{(double)x, (double)y, (double)z}, du, dv);
-        const int iu = (int)floor(du + 0.5), iv = (int)floor(dv + 0.5);
-        if (iu < 0 || iu >= (int)P.nu || iv < 0 || iv >= (int)P.nv) return 0.f;
-        return __ldg(pv + (iu * P.su + iv * P.sv));
-    }
-    const float gu = floorf(fu + 0.5f), gv = floorf(fv + 0.5f);
-    if (!(gu >= 0.f && gu < (float)P.nu && gv >= 0.f && gv < (float)P.nv)) return 0.f;
-    return __ldg(pv + ((int)gu * P.su + (int)gv * P.sv));
+__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pvw, int view, float fu, float fv,
+                                               const VoxRef &r) {
+    const float gu = fu + 0.5f, gv = fv + 0.5f;
+    const float lu = floorf(gu), lv = floorf(gv);
+    // |frac - 1/2| <= 1/2 - kRefine on both axes, written so that NaN fails
+    if (!(fabsf(gu - lu - 0.5f) <= 0.5f - kRefine && fabsf(gv - lv - 0.5f) <= 0.5f - kRefine))
+        return refine_nearest(P, pvw, view, r);
+    // float -> int saturates, so out-of-range values fail the unsigned test
+    const int iu = (int)lu, iv = (int)lv;
+    if ((unsigned)iu >= P.nu || (unsigned)iv >= P.nv) return 0.f;
+    return __ldg(pvw + (iu * P.su + iv * P.sv));
 }
 
 // Bilinear rule of get_bilinear_interp (CB_backproject.cu:221-254), same
 // operation order.
-__device__ __forceinline__ float fetch_bilinear(const BPParams &P, const float *pv, float fu, float fv) {
+__device__ __forceinline__ float fetch_bilinear(const BPParams &P, const float *pvw, float fu, float fv) {
     if (fu <= -1.f || fv <= -1.f || fu >= (float)P.nu || fv >= (float)P.nv) return 0.f;
     const int i0 = (int)floorf(fu), j0 = (int)floorf(fv);
     const float fx = fu - (float)i0, fy = fv - (float)j0;
     auto get = [&](int i, int j) -> float {
         if (i < 0 || i >= (int)P.nu || j < 0 || j >= (int)P.nv) return 0.f;
-        return __ldg(pv + (i * P.su + j * P.sv));
+        return __ldg(pvw + (i * P.su + j * P.sv));
     };
     const float v00 = get(i0, j0), v01 = get(i0, j0 + 1), v10 = get(i0 + 1, j0), v11 = get(i0 + 1, j0 + 1);
     const float t1 = v00 * (1.f - fx) + v10 * fx;
@@ -96,19 +116,49 @@ __device__ __forceinline__ float dot4(const float4 a, float x, float y, float z)
     return fmaf(a.x, x, fmaf(a.y, y, fmaf(a.z, z, a.w)));
 }
 
+// 1/x with one MUFU op (relative error < 2^-22); nearest-pixel ties are
+// settled in FP64 separately.
+__device__ __forceinline__ float rcp_fast(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float taper(const ab_bpview &b, float fu, float fv, float inv_sep) {
+    if (fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv) return 1.f;
+    return ab_edge_taper(fu - b.cu0, fv - b.cv0, b.inv_halfu, b.inv_halfv, inv_sep);
+}
+
+__device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, float Z) {
+    float w = 1.f;
+    if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
+    if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
+    return w;
+}
+
 // EXACT: chord-length footprint (CB_backproject.cu:408-477).
 // RAYCAST: fast mode with direct-raycast weights (:512-646, preset 0).
 // BILIN: bilinear instead of nearest detector sampling.
 // ORD: 0 = C order (fastest axis z, slowest x), 1 = F order (fastest x).
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
-__global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
+__global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
     __shared__ ab_bpview sv[kChunk];
     __shared__ ab_bpview_exact sx[EXACT ? kChunk : 1];
 
+    // Brick-ordered block coordinates (uniform per CTA).
+    const int per_sb = P.gb[0] * P.sb1 * P.sb2;
+    const int sb = blockIdx.x / per_sb;
+    int r = blockIdx.x - sb * per_sb;
+    const int b0 = r % P.gb[0];
+    r /= P.gb[0];
+    const int b1 = (sb % P.nsb1) * P.sb1 + r % P.sb1;
+    const int b2 = (sb / P.nsb1) * P.sb2 + r / P.sb1;
+    if (b1 >= P.gb[1] || b2 >= P.gb[2]) return;  // the whole CTA exits before any barrier
+
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i0 = blockIdx.x * 32 + lane;
-    const int i1 = blockIdx.y * 8 + warp;
-    const int i2b = blockIdx.z * kXB;
+    const int i0 = b0 * 32 + lane;
+    const int i1 = b1 * 8 + warp;
+    const int i2b = b2 * kXB;
     constexpr int a0 = ORD == 0 ? 2 : 0, a1 = 1, a2 = ORD == 0 ? 0 : 2;
     const bool in01 = i0 < P.n[a0] && i1 < P.n[a1];
 
@@ -122,9 +172,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) base[a] = ((float)idx[a] + 0.5f - 0.5f * (float)P.n[a]) * vw;
 
-    // Cylinder mask about world x = y = 0 (CB_backproject.cu:339-343); it
-    // depends on x and y only, so it may differ between the XB voxels when the
-    // slowest axis is x or y.
+    // Cylinder mask about world x = y = 0 (CB_backproject.cu:339-343).
     bool live[kXB];
     bool any_live = false;
 #pragma unroll
@@ -140,34 +188,32 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
         any_live |= ok;
     }
 
-    float acc_x[kXB];
+    // One accumulator per voxel over all views and sub-samples; the mean over
+    // the ssx*ssy*ssz sub-samples is taken at the end (the reference averages
+    // level by level, CB_backproject.cu:717-731 -- the same value up to float
+    // rounding, identical when there is no supersampling).
+    float acc[kXB];
 #pragma unroll
-    for (int k = 0; k < kXB; ++k) acc_x[k] = 0.f;
+    for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
 
     const ab_d3 c0d{(double)P.c0[0], (double)P.c0[1], (double)P.c0[2]};
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
-    for (int si = 0; si < P.ssx; ++si) {
-        float acc_y[kXB];
-#pragma unroll
-        for (int k = 0; k < kXB; ++k) acc_y[k] = 0.f;
-        for (int sj = 0; sj < P.ssy; ++sj) {
-            float acc_z[kXB];
-#pragma unroll
-            for (int k = 0; k < kXB; ++k) acc_z[k] = 0.f;
-            for (int sk = 0; sk < P.ssz; ++sk) {
-                const float sub[3] = {(-0.5f + offx * (0.5f + si)) * vw, (-0.5f + offy * (0.5f + sj)) * vw,
-                                      (-0.5f + offz * (0.5f + sk)) * vw};
-                float acc[kXB];
-#pragma unroll
-                for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
-                const float X0 = base[0] + sub[0], Y0 = base[1] + sub[1], Z0 = base[2] + sub[2];
+    const bool needZ = P.pL != 0 || P.pV != 0;
+    const int n_sub = P.ssx * P.ssy * P.ssz;
+    for (int isub = 0; isub < n_sub; ++isub) {
+        const int si = isub / (P.ssy * P.ssz), sj = (isub / P.ssz) % P.ssy, sk = isub % P.ssz;
+        {
+            {
+                const float fsub[3] = {-0.5f + offx * (0.5f + si), -0.5f + offy * (0.5f + sj),
+                                       -0.5f + offz * (0.5f + sk)};
+                const float X0 = base[0] + fsub[0] * vw, Y0 = base[1] + fsub[1] * vw, Z0 = base[2] + fsub[2] * vw;
 
                 for (uint32_t v0 = 0; v0 < P.n_views; v0 += kChunk) {
                     const int cn = (int)min((uint32_t)kChunk, P.n_views - v0);
                     __syncthreads();
                     for (int t = threadIdx.x; t < cn; t += kThreads) {
                         const aprict_proj_spec sp = P.specs[v0 + t];
-                        if (!ab_derive_bpview(sp, c0d, vw, sv[t]) && P.status)
+                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t]) && P.status)
                             atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
                     }
@@ -176,13 +222,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                     for (int t = 0; t < cn; ++t) {
                         const int view = (int)v0 + t;
                         const ab_bpview b = sv[t];
-                        const float *pvw = P.projs + (int64_t)view * P.ps.view;
+                        const float *pvw = P.projs + (int64_t)view * P.stride_view;
                         const float Nu0 = dot4(b.nu, X0, Y0, Z0), Nv0 = dot4(b.nv, X0, Y0, Z0);
                         const float D0 = dot4(b.den, X0, Y0, Z0);
                         const float dNu = (a2 == 0 ? b.nu.x : (a2 == 1 ? b.nu.y : b.nu.z)) * vw;
                         const float dNv = (a2 == 0 ? b.nv.x : (a2 == 1 ? b.nv.y : b.nv.z)) * vw;
                         const float dD = (a2 == 0 ? b.den.x : (a2 == 1 ? b.den.y : b.den.z)) * vw;
-                        const bool needZ = RAYCAST ? (P.pL != 0 || P.pV != 0) : (P.pL != 0 || P.pV != 0);
                         float Zb = 0.f, dZ = 0.f;
                         if (needZ) {
                             Zb = dot4(b.zl, X0, Y0, Z0);
@@ -193,7 +238,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                             if (!live[k]) continue;
                             const float kf = (float)k;
                             const float D = fmaf(kf, dD, D0);
-                            const float rD = __frcp_rn(D);
+                            const float rD = rcp_fast(D);
                             const float fu = fmaf(kf, dNu, Nu0) * rD;
                             const float fv = fmaf(kf, dNv, Nv0) * rD;
                             float s;
@@ -211,9 +256,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                     const float sx_ = (c & 4) ? 1.f : -1.f, sy_ = (c & 2) ? 1.f : -1.f,
                                                 sz_ = (c & 1) ? 1.f : -1.f;
                                     const float dd = D + sx_ * hd[0] + sy_ * hd[1] + sz_ * hd[2];
-                                    const float r = 1.f / dd;
-                                    const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * r;
-                                    const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * r;
+                                    const float rr = rcp_fast(dd);
+                                    const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * rr;
+                                    const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * rr;
                                     umin = fminf(umin, uu);
                                     umax = fmaxf(umax, uu);
                                     vmin = fminf(vmin, vv);
@@ -239,7 +284,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                         float a_lo = 0.f, a_hi = 3.0e38f;
                                         bool miss = false;
                                         if (dx != 0.f) {
-                                            const float inv = __frcp_rn(dx);
+                                            const float inv = rcp_fast(dx);
                                             const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -247,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                             miss |= fabsf(r0x) > h;
                                         }
                                         if (dy != 0.f) {
-                                            const float inv = __frcp_rn(dy);
+                                            const float inv = rcp_fast(dy);
                                             const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -255,7 +300,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                             miss |= fabsf(r0y) > h;
                                         }
                                         if (dz != 0.f) {
-                                            const float inv = __frcp_rn(dz);
+                                            const float inv = rcp_fast(dz);
                                             const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
                                             a_lo = fmaxf(a_lo, fminf(t1, t2));
                                             a_hi = fminf(a_hi, fmaxf(t1, t2));
@@ -268,76 +313,53 @@ __global__ void __launch_bounds__(kThreads, 2) k_backproject(BPParams P) {
                                         s = fmaf(pv, chord, s);
                                     }
                                 }
-                                if (needZ) {
-                                    const float Z = fmaf(kf, dZ, Zb);
-                                    if (P.pL != 0) s *= ab_powint(Z * b.invL, P.pL);
-                                    if (P.pV != 0) s *= ab_powint(Z / P.val, P.pV);
-                                }
+                                if (needZ) s *= zpow(P, b, fmaf(kf, dZ, Zb));
                             } else {
-                                float w;
-                                if (RAYCAST) {
-                                    w = 1.f;
-                                    if (needZ) {
-                                        const float Z = fmaf(kf, dZ, Zb);
-                                        if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
-                                        if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
-                                    }
-                                } else {
-                                    // (|p - s| / |x - s|)^2 * voxwid^3 / pixel area (:648-690)
-                                    w = b.kfast * rD * rD;
-                                    if (needZ) {
-                                        const float Z = fmaf(kf, dZ, Zb);
-                                        if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
-                                        if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
-                                    }
-                                }
+                                // fast mode: weight (|p - s| / |x - s|)^2 voxwid^3 / pixel area
+                                // (:648-690), or the direct-raycast weights (:512-646)
+                                float w = RAYCAST ? 1.f : b.kfast * rD * rD;
+                                if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
                                 float pv = 0.f;
                                 if (w != 0.f) {
                                     if (BILIN) {
                                         pv = fetch_bilinear(P, pvw, fu, fv);
                                     } else {
-                                        float xw[3] = {X0 + P.c0[0], Y0 + P.c0[1], Z0 + P.c0[2]};
-                                        xw[a2] += kf * vw;
-                                        pv = fetch_nearest(P, pvw, view, fu, fv, xw[0], xw[1], xw[2]);
+                                        int id[3];
+                                        id[a0] = i0;
+                                        id[a1] = i1;
+                                        id[a2] = i2b + k;
+                                        const VoxRef vr{id[0], id[1], id[2], fsub[0], fsub[1], fsub[2]};
+                                        pv = fetch_nearest(P, pvw, view, fu, fv, vr);
                                     }
                                 }
                                 s = pv * w;
                             }
-                            if (P.sep > 0.f && s != 0.f) {
-                                s *= ab_edge_taper(fu - (b.halfu - 0.5f), fv - (b.halfv - 0.5f), b.inv_halfu, b.inv_halfv,
-                                                   P.inv_sep);
-                            }
+                            if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
                             acc[k] += s;
                         }
                     }
                 }
-#pragma unroll
-                for (int k = 0; k < kXB; ++k) acc_z[k] += acc[k];
             }
-#pragma unroll
-            for (int k = 0; k < kXB; ++k) acc_y[k] += acc_z[k] / (float)P.ssz;
         }
-#pragma unroll
-        for (int k = 0; k < kXB; ++k) acc_x[k] += acc_y[k] / (float)P.ssy;
     }
 
 #pragma unroll
     for (int k = 0; k < kXB; ++k) {
         if (!live[k]) continue;
-        const float value = acc_x[k] / (float)P.ssx;
+        const float value = n_sub == 1 ? acc[k] : acc[k] / (float)n_sub;
         if (value == 0.f) continue;  // the reference skips the write (:1010)
         int id[3];
         id[a0] = i0;
         id[a1] = i1;
         id[a2] = i2b + k;
         const int64_t o = (int64_t)id[0] * P.vs[0] + (int64_t)id[1] * P.vs[1] + (int64_t)id[2] * P.vs[2];
-        const float m = P.mult ? P.mult[o] : 1.f;
-        P.vol[o] = value * m + P.vol[o];
+        const float m = P.mult ? __ldcs(P.mult + o) : 1.f;
+        __stcs(P.vol + o, value * m + __ldcs(P.vol + o));
     }
 }
 
 template <int ORD>
-void launch_bp(const BPParams &P, const aprict_backproject_config *cfg, bool lin, dim3 grid, cudaStream_t st) {
+void launch_bp(const BPParams &P, const aprict_backproject_config *cfg, bool lin, unsigned grid, cudaStream_t st) {
     if (cfg->exact) {
         k_backproject<ORD, true, false, false><<<grid, kThreads, 0, st>>>(P);
     } else if (cfg->approx_mode_direct_raycast) {
@@ -377,18 +399,18 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     if (specs_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null view specs");
     if (multiplier_dev && (reinterpret_cast<uintptr_t>(multiplier_dev) & 3u))
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "multiplier pointer not 4-byte aligned");
+    if ((int64_t)(pd->nu - 1) * pd->stride_u + (int64_t)(pd->nv - 1) * pd->stride_v + 1 > 0x7fffffffLL)
+        return ab_fail(APRICT_ERR_TOO_LARGE, "one projection image spans more than 2^31 elements");
 
     BPParams P{};
     P.specs = specs_dev;
     P.n_views = pd->n_views;
     P.nu = pd->nu;
     P.nv = pd->nv;
-    P.ps = ab_pstrides{pd->stride_view, pd->stride_u, pd->stride_v};
-    P.projs = projs_dev;
+    P.stride_view = pd->stride_view;
     P.su = (int)pd->stride_u;
     P.sv = (int)pd->stride_v;
-    if ((int64_t)(pd->nu - 1) * pd->stride_u + (int64_t)(pd->nv - 1) * pd->stride_v + 1 > 0x7fffffffLL)
-        return ab_fail(APRICT_ERR_TOO_LARGE, "one projection image spans more than 2^31 elements");
+    P.projs = projs_dev;
     P.vol = vol_dev;
     P.mult = multiplier_dev;
     P.n[0] = (int)vd->nx;
@@ -404,6 +426,10 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
         P.vs[2] = (int64_t)vd->nx * vd->ny;
     }
     P.voxwid = vd->voxwid;
+    P.vwd = (double)vd->voxwid;
+    P.cornerd[0] = vd->corner.x;
+    P.cornerd[1] = vd->corner.y;
+    P.cornerd[2] = vd->corner.z;
     P.c0[0] = vd->corner.x + 0.5f * vd->voxwid * (float)vd->nx;
     P.c0[1] = vd->corner.y + 0.5f * vd->voxwid * (float)vd->ny;
     P.c0[2] = vd->corner.z + 0.5f * vd->voxwid * (float)vd->nz;
@@ -421,13 +447,34 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.status = status_dev;
 
     const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
-    dim3 grid((unsigned)((n0 + 31) / 32), (unsigned)((n1 + 7) / 8), (unsigned)((n2 + kXB - 1) / kXB));
-    if (grid.y > 65535u || grid.z > 65535u) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
+    P.gb[0] = (n0 + 31) / 32;
+    P.gb[1] = (n1 + 7) / 8;
+    P.gb[2] = (n2 + kXB - 1) / kXB;
+    // Super-brick: all blocks of the fastest axis x sb1 x sb2 blocks (8 and
+    // kXB voxels each), about one wave of resident CTAs, with equal extents in
+    // voxels along the middle and slowest axes.
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    }
+    const double target = 3.0 * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
+    int sb1 = (int)floor(sqrt(target * kXB / 8.0) + 0.5);
+    sb1 = sb1 < 1 ? 1 : (sb1 > P.gb[1] ? P.gb[1] : sb1);
+    int sb2 = (int)floor(target / sb1 + 0.5);
+    sb2 = sb2 < 1 ? 1 : (sb2 > P.gb[2] ? P.gb[2] : sb2);
+    P.sb1 = sb1;
+    P.sb2 = sb2;
+    P.nsb1 = (P.gb[1] + sb1 - 1) / sb1;
+    const int64_t nsb = (int64_t)P.nsb1 * ((P.gb[2] + sb2 - 1) / sb2);
+    const int64_t grid = nsb * P.gb[0] * sb1 * sb2;
+    if (grid > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const bool lin = cfg->approx_mode_linear_interpolate != 0;
     if (vd->order == 0)
-        launch_bp<0>(P, cfg, lin, grid, st);
+        launch_bp<0>(P, cfg, lin, (unsigned)grid, st);
     else
-        launch_bp<1>(P, cfg, lin, grid, st);
+        launch_bp<1>(P, cfg, lin, (unsigned)grid, st);
     return ab_cuda_check(cudaGetLastError(), "backproject launch");
 }

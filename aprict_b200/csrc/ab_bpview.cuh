@@ -30,6 +30,9 @@ struct ab_bpview {
     float halfu; // nu / 2
     float halfv; // nv / 2
     float inv_halfu, inv_halfv;
+    // Edge taper: |fu - cu0| <= tap_ru and |fv - cv0| <= tap_rv guarantees a
+    // factor of exactly 1 (a margin of 1e-5 keeps it conservative).
+    float cu0, cv0, tap_ru, tap_rv;
 };
 
 // Exact-mode extras: ray origin and per-pixel direction in world units,
@@ -41,7 +44,7 @@ struct ab_bpview_exact {
     float4 v;   // det_v
 };
 
-AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, ab_bpview &o) {
+AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, float sep, ab_bpview &o) {
     const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
     const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);
     const ab_d3 n = ab_cross(U, V);
@@ -72,6 +75,11 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     o.halfv = (float)sp.nv * 0.5f;
     o.inv_halfu = (float)(2.0 / (double)sp.nu);
     o.inv_halfv = (float)(2.0 / (double)sp.nv);
+    o.cu0 = (float)hu;
+    o.cv0 = (float)hv;
+    const double keep = sep > 0.f ? (1.0 - (double)sep) * (1.0 - 1e-5) : 1e30;
+    o.tap_ru = (float)(0.5 * (double)sp.nu * keep);
+    o.tap_rv = (float)(0.5 * (double)sp.nv * keep);
     return true;
 }
 

@@ -97,6 +97,8 @@ size_t aprict_b200_struct_size(const char *name) {
     if (!strcmp(name, "aprict_proj_desc")) return sizeof(aprict_proj_desc);
     if (!strcmp(name, "aprict_project_config")) return sizeof(aprict_project_config);
     if (!strcmp(name, "aprict_backproject_config")) return sizeof(aprict_backproject_config);
+    if (!strcmp(name, "aprict_forbild_shape")) return sizeof(aprict_forbild_shape);
+    if (!strcmp(name, "aprict_quadric")) return sizeof(aprict_quadric);
     return 0;
 }
 

@@ -93,10 +93,21 @@ AB_HD ab_d3 ab_to_grid(const ab_grid<Off> &g, ab_d3 p) {
 // the voxel is ceil(c)-1 (reference :189-203, :244-246), so a ray lying in the
 // plane c == 0 misses and one in c == n hits the last layer.
 //
-// Returns false (visiting nothing) when the segment misses the grid or its
-// input is not finite; *bad is set for non-finite input.
-template <typename Off, class Visit>
-AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visit &visit, bool *bad) {
+// ab_siddon_setup prepares the traversal state (in FP64, then rounded to the
+// FP32 stepping quantities); ab_siddon runs it with a visitor. Both return
+// false when the segment misses the grid or its input is not finite (*bad is
+// set for non-finite input).
+template <typename Off>
+struct ab_ray {
+    float t0x, t0y, t0z;  // first crossing along each axis (from the entry point)
+    float dtx, dty, dtz;  // crossing spacing along each axis
+    float tend;           // exit, clamped to every axis's last in-grid crossing
+    Off off;              // element offset of the entry voxel
+    Off ox, oy, oz;       // signed element steps
+};
+
+template <typename Off>
+AB_HD bool ab_siddon_setup(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], ab_ray<Off> &r, bool *bad) {
     if (!ab_finite3(o) || !ab_finite3(e)) {
         *bad = true;
         return false;
@@ -119,8 +130,8 @@ AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visi
     if (!(a_in < a_out)) return false;
     const double len = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
 
-    int idx[3], lim[3], stp[3];
-    float t0f[3], dtf[3];
+    int stp[3];
+    float t0f[3], dtf[3], texit[3];
     Off off = 0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -132,59 +143,112 @@ AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visi
             i = (int)ceil(p) - 1;
         }
         i = i < 0 ? 0 : (i >= n[a] ? n[a] - 1 : i);
-        idx[a] = i;
         off += (Off)i * stride[a];
         if (dd[a] == 0.0) {
             stp[a] = 0;
-            lim[a] = -2;  // never reached
             t0f[a] = INFINITY;
             dtf[a] = 0.f;
+            texit[a] = INFINITY;
         } else {
             const bool pos = dd[a] > 0.0;
             stp[a] = pos ? 1 : -1;
-            lim[a] = pos ? n[a] : -1;
             const double b = pos ? (double)(i + 1) : (double)i;
             const double ab = (b - od[a]) / dd[a];
             t0f[a] = (float)((ab - a_in) * len);
             dtf[a] = (float)(len / fabs(dd[a]));
+            // Crossings left along this axis until the grid boundary; the last
+            // one (k = K-1) is evaluated with the loop's own fma.
+            const int K = pos ? n[a] - i : i + 1;
+            texit[a] = fmaf((float)(K - 1), dtf[a], t0f[a]);
         }
     }
-    const float tend = (float)((a_out - a_in) * len);
-    // Scalars (not arrays) in the loop keep everything in registers.
-    int ix = idx[0], iy = idx[1], iz = idx[2];
-    const int lx = lim[0], ly = lim[1], lz = lim[2];
-    const Off ox = stp[0] > 0 ? stride[0] : (Off)0 - stride[0];
-    const Off oy = stp[1] > 0 ? stride[1] : (Off)0 - stride[1];
-    const Off oz = stp[2] > 0 ? stride[2] : (Off)0 - stride[2];
-    const int sx = stp[0], sy = stp[1], sz = stp[2];
-    const float t0x = t0f[0], t0y = t0f[1], t0z = t0f[2];
-    const float dtx = dtf[0], dty = dtf[1], dtz = dtf[2];
+    // The loop stops at tend. Clamping tend to every axis's boundary crossing,
+    // computed by the same fma the loop uses (bitwise identical values), makes
+    // a step past the last voxel along any axis impossible: that step would
+    // need tm == texit[a] < tend <= texit[a]. No index bookkeeping is needed.
+    r.tend = fminf((float)((a_out - a_in) * len), fminf(texit[0], fminf(texit[1], texit[2])));
+    r.off = off;
+    r.ox = stp[0] > 0 ? stride[0] : (Off)0 - stride[0];
+    r.oy = stp[1] > 0 ? stride[1] : (Off)0 - stride[1];
+    r.oz = stp[2] > 0 ? stride[2] : (Off)0 - stride[2];
+    r.t0x = t0f[0];
+    r.t0y = t0f[1];
+    r.t0z = t0f[2];
+    r.dtx = dtf[0];
+    r.dty = dtf[1];
+    r.dtz = dtf[2];
+    return true;
+}
+
+// One traversal step: tm is the next crossing; advances the state past it.
+// Branch-free: every lane of a warp runs the same instructions whichever axis
+// its ray crosses next. The three crossings are recomputed from their
+// counters (an unchanged counter reproduces the same value), so no per-axis
+// selects are needed.
+#define AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm) \
+    do {                                                      \
+        const bool bx_ = (tx) == (tm);                        \
+        const bool by_ = !bx_ && ((ty) == (tm));              \
+        (off) += bx_ ? (R).ox : (by_ ? (R).oy : (R).oz);      \
+        (kx) += bx_ ? 1.f : 0.f;                              \
+        (ky) += by_ ? 1.f : 0.f;                              \
+        (kz) += (bx_ || by_) ? 0.f : 1.f;                     \
+        (tx) = fmaf((kx), (R).dtx, (R).t0x);                  \
+        (ty) = fmaf((ky), (R).dty, (R).t0y);                  \
+        (tz) = fmaf((kz), (R).dtz, (R).t0z);                  \
+    } while (0)
+
+// Visits every (segment length in voxel units, element offset) of the ray.
+template <typename Off, class Visit>
+AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visit &visit, bool *bad) {
+    ab_ray<Off> R;
+    if (!ab_siddon_setup<Off>(o, e, n, stride, R, bad)) return false;
+    Off off = R.off;
     float kx = 0.f, ky = 0.f, kz = 0.f;
-    float tx = t0x, ty = t0y, tz = t0z;
+    float tx = R.t0x, ty = R.t0y, tz = R.t0z;
     float t = 0.f;
-    // Branch-free step: every lane of a warp runs the same instructions
-    // whichever axis its ray crosses next (a 3-way branch would serialise).
     for (;;) {
         const float tm = fminf(tx, fminf(ty, tz));
-        const float te = fminf(tm, tend);
-        visit(te - t, off);
-        if (tm >= tend) break;
+        visit(fminf(tm, R.tend) - t, off);
+        if (tm >= R.tend) break;
         t = tm;
-        const bool bx = tx == tm;
-        const bool by = !bx && (ty == tm);
-        const bool bz = !bx && !by;
-        off += bx ? ox : (by ? oy : oz);
-        ix += bx ? sx : 0;
-        iy += by ? sy : 0;
-        iz += bz ? sz : 0;
-        if ((ix == lx) | (iy == ly) | (iz == lz)) break;
-        kx += bx ? 1.f : 0.f;
-        ky += by ? 1.f : 0.f;
-        kz += bz ? 1.f : 0.f;
-        tx = bx ? fmaf(kx, dtx, t0x) : tx;
-        ty = by ? fmaf(ky, dty, t0y) : ty;
-        tz = bz ? fmaf(kz, dtz, t0z) : tz;
+        AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm);
     }
+    return true;
+}
+
+// Line integral sum(seg * vol[off]) (voxel units), Kahan-compensated, with the
+// gather of the next voxel issued before the current one is accumulated so
+// that one load is always in flight. load(off) must be a pure read.
+template <typename Off, class Load>
+AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Load &load, float &sum,
+                            bool *bad) {
+    ab_ray<Off> R;
+    sum = 0.f;
+    if (!ab_siddon_setup<Off>(o, e, n, stride, R, bad)) return false;
+    Off off = R.off;
+    float kx = 0.f, ky = 0.f, kz = 0.f;
+    float tx = R.t0x, ty = R.t0y, tz = R.t0z;
+    float t = 0.f, s = 0.f, c = 0.f;
+    float mu = load(off);
+    for (;;) {
+        const float tm = fminf(tx, fminf(ty, tz));
+        const float seg = fminf(tm, R.tend) - t;
+        if (tm >= R.tend) {
+            const float y = seg * mu - c;
+            s += y;
+            break;
+        }
+        t = tm;
+        AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm);
+        const float mu_next = load(off);  // in the grid: the loop did not stop
+        const float y = seg * mu - c;
+        const float tt = s + y;
+        c = (tt - s) - y;
+        s = tt;
+        mu = mu_next;
+    }
+    sum = s;
     return true;
 }
 

@@ -35,9 +35,16 @@ TileMap make_tiles(uint32_t nu, uint32_t nv) {
     return t;
 }
 
-__device__ __forceinline__ void tile_pixel(const TileMap &tm, int tile, int &iu, int &iv) {
-    const int tu = tile % tm.ntu;
-    const int tv = tile / tm.ntu;
+// Blocks are ordered (detector row band, view, column tile) with the band
+// slowest: the CTAs resident at one time work on one band of rows of some
+// tens of views, whose rays cross only a slab of the volume, so the volume
+// data they gather stays in L2 (rather than whole views, which touch all of it).
+__device__ __forceinline__ void block_tile(const TileMap &tm, uint32_t n_views, int &view, int &iu, int &iv) {
+    const uint32_t b = blockIdx.x;
+    const int tu = (int)(b % (uint32_t)tm.ntu);
+    const uint32_t rest = b / (uint32_t)tm.ntu;
+    view = (int)(rest % n_views);
+    const int tv = (int)(rest / n_views);
     const int t = threadIdx.x;
     if (tm.tile_v == 1) {
         iu = tu * tm.tile_u + t;
@@ -51,11 +58,26 @@ __device__ __forceinline__ void tile_pixel(const TileMap &tm, int tile, int &iu,
     }
 }
 
+// L2 policy for the volume gathers: keep the volume resident (evict_last)
+// while the streamed projection reads/writes of the same kernel are marked
+// evict-first, so a volume that fits in L2 is fetched from HBM about once.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ float ldg_keep(const float *p, uint64_t pol) {
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 template <typename Off>
-struct GatherVisit {
+struct VolLoad {
     const float *__restrict__ vol;
-    ab_kahan acc;
-    __device__ __forceinline__ void operator()(float seg, Off off) { acc.add(seg * __ldg(vol + off)); }
+    uint64_t pol;
+    __device__ __forceinline__ float operator()(Off off) const { return ldg_keep(vol + off, pol); }
 };
 
 template <typename Off>
@@ -72,17 +94,16 @@ template <typename Off>
 __global__ void __launch_bounds__(kThreads, 4)
     k_project_siddon(const aprict_proj_spec *__restrict__ specs, uint32_t n_views, uint32_t nu, uint32_t nv,
                      ab_pstrides ps, float *__restrict__ out, const float *base, ab_grid<Off> g, const float *vol,
-                     float svf, float mba, int ssu, int ssv, TileMap tm, uint32_t view0, uint32_t *status) {
-    const uint32_t view = view0 + blockIdx.y;
-    if (view >= n_views) return;
-    int iu, iv;
-    tile_pixel(tm, blockIdx.x, iu, iv);
+                     float svf, float mba, int ssu, int ssv, TileMap tm, uint32_t *status) {
+    int view, iu, iv;
+    block_tile(tm, n_views, view, iu, iv);
     if (iu >= (int)nu || iv >= (int)nv) return;
     const aprict_proj_spec sp = specs[view];
     const ab_d3 src = ab_to_grid(g, ab_d3_of(sp.source_pos) * (double)svf);
 
     bool bad = false;
     float tot = 0.f;
+    const uint64_t pol = l2_evict_last_policy();
     const double inv_su = 1.0 / (double)ssu, inv_sv = 1.0 / (double)ssv;
     for (int ku = 0; ku < ssu; ++ku) {
         float accu = 0.f;
@@ -90,9 +111,10 @@ __global__ void __launch_bounds__(kThreads, 4)
             const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
             const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
             const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)svf);
-            GatherVisit<Off> vis{vol, {0.f, 0.f}};
-            ab_siddon<Off>(src, dst, g.n, g.stride, vis, &bad);
-            accu += (vis.acc.s * g.voxwid) * mba;
+            VolLoad<Off> ld{vol, pol};
+            float sum;
+            ab_siddon_gather<Off>(src, dst, g.n, g.stride, ld, sum, &bad);
+            accu += (sum * g.voxwid) * mba;
         }
         if (ssv > 1) accu /= (float)ssv;
         tot += accu;
@@ -101,7 +123,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (bad && status) atomicOr(status, APRICT_STATUS_NONFINITE);
     const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
     if (base) {
-        out[o] = base[o] + tot;
+        __stcs(out + o, __ldcs(base + o) + tot);  // streamed once: evict-first
     } else {
         atomicAdd(out + o, tot);
     }
@@ -111,11 +133,9 @@ template <typename Off>
 __global__ void __launch_bounds__(kThreads, 4)
     k_backproject_scatter(const aprict_proj_spec *__restrict__ specs, uint32_t n_views, uint32_t nu, uint32_t nv,
                           ab_pstrides ps, const float *__restrict__ projs, ab_grid<Off> g, float *vol, float svf,
-                          float mba, int ssu, int ssv, TileMap tm, uint32_t view0, uint32_t *status) {
-    const uint32_t view = view0 + blockIdx.y;
-    if (view >= n_views) return;
-    int iu, iv;
-    tile_pixel(tm, blockIdx.x, iu, iv);
+                          float mba, int ssu, int ssv, TileMap tm, uint32_t *status) {
+    int view, iu, iv;
+    block_tile(tm, n_views, view, iu, iv);
     if (iu >= (int)nu || iv >= (int)nv) return;
     const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
     const float p = projs[o];
@@ -168,24 +188,18 @@ extern "C" int aprict_b200_project_siddon(const aprict_proj_spec *specs_dev, con
     const TileMap tm = make_tiles(pd->nu, pd->nv);
     const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    for (uint32_t v0 = 0; v0 < pd->n_views; v0 += 65535u) {
-        const uint32_t nvw = pd->n_views - v0 < 65535u ? pd->n_views - v0 : 65535u;
-        dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
-        if (small_volume(vd)) {
-            k_project_siddon<int32_t><<<grid, kThreads, 0, st>>>(
-                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int32_t>(*vd),
-                vol_dev, cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm,
-                v0, status_dev);
-        } else {
-            k_project_siddon<int64_t><<<grid, kThreads, 0, st>>>(
-                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int64_t>(*vd),
-                vol_dev, cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm,
-                v0, status_dev);
-        }
-        rc = ab_cuda_check(cudaGetLastError(), "project_siddon launch");
-        if (rc != APRICT_OK) return rc;
+    const uint64_t nblocks = (uint64_t)tm.ntu * tm.ntv * pd->n_views;
+    if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
+    if (small_volume(vd)) {
+        k_project_siddon<int32_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
+            specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int32_t>(*vd), vol_dev,
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
+    } else {
+        k_project_siddon<int64_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
+            specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, base_dev, ab_make_grid<int64_t>(*vd), vol_dev,
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
     }
-    return APRICT_OK;
+    return ab_cuda_check(cudaGetLastError(), "project_siddon launch");
 }
 
 extern "C" int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
@@ -198,22 +212,16 @@ extern "C" int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev
     const TileMap tm = make_tiles(pd->nu, pd->nv);
     const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    for (uint32_t v0 = 0; v0 < pd->n_views; v0 += 65535u) {
-        const uint32_t nvw = pd->n_views - v0 < 65535u ? pd->n_views - v0 : 65535u;
-        dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
-        if (small_volume(vd)) {
-            k_backproject_scatter<int32_t><<<grid, kThreads, 0, st>>>(
-                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int32_t>(*vd), vol_dev,
-                cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, v0,
-                status_dev);
-        } else {
-            k_backproject_scatter<int64_t><<<grid, kThreads, 0, st>>>(
-                specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int64_t>(*vd), vol_dev,
-                cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, v0,
-                status_dev);
-        }
-        rc = ab_cuda_check(cudaGetLastError(), "backproject_scatter launch");
-        if (rc != APRICT_OK) return rc;
+    const uint64_t nblocks = (uint64_t)tm.ntu * tm.ntv * pd->n_views;
+    if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
+    if (small_volume(vd)) {
+        k_backproject_scatter<int32_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
+            specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int32_t>(*vd), vol_dev,
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
+    } else {
+        k_backproject_scatter<int64_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
+            specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int64_t>(*vd), vol_dev,
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
     }
-    return APRICT_OK;
+    return ab_cuda_check(cudaGetLastError(), "backproject_scatter launch");
 }

@@ -95,3 +95,62 @@ def ellipsoid_volume(
     """A seeded additive random-ellipsoid volume (the workloads' phantom)."""
     rng = np.random.default_rng(seed)
     return voxelize(random_ellipsoids(rng, n, shape=shape, voxwid=voxwid, semi_axes_vox=semi_axes_vox, rho=rho), shape, voxwid)
+
+
+def _unit(v: np.ndarray) -> np.ndarray:
+    return v / np.linalg.norm(v)
+
+
+def random_quadric_phantom(
+    seed: int,
+    *,
+    n_ellipsoids: int = 60,
+    n_cylinders: int = 40,
+    radius: float = 100.0,
+    rho: tuple[float, float] = (-0.2, 1.0),
+    size: tuple[float, float] = (5.0, 40.0),
+    max_clips: int = 3,
+) -> np.ndarray:
+    """FORBILD_Shape records: free ellipsoids (type 11) then elliptic cylinders (type 12).
+
+    Each shape has 0..max_clips random clip planes through a point near its
+    centre, a density uniform in ``rho``, and lies inside a sphere of
+    ``radius`` (the quadric-phantom workload: 60 + 40 shapes in 200 mm).
+    """
+    from ._structs import forbild_shape  # noqa: PLC0415
+
+    rng = np.random.default_rng(seed)
+    n = n_ellipsoids + n_cylinders
+    out = np.zeros(n, dtype=forbild_shape)
+    for i in range(n):
+        frame = random_rotation(rng)
+        semi = rng.uniform(size[0], size[1], size=3)
+        ext = float(np.max(semi))
+        if i >= n_ellipsoids:
+            ext = float(np.hypot(max(semi[0], semi[1]), semi[2]))
+        dist = rng.uniform(0, max(radius - ext, 0.0))
+        c = _unit(rng.standard_normal(3)) * dist
+        rec = out[i]
+        rec["rho"] = rng.uniform(*rho)
+        rec["x"], rec["y"], rec["z"] = c
+        if i < n_ellipsoids:
+            rec["type"] = 11
+            rec["dx"], rec["dy"], rec["dz"] = semi
+            rec["a_x"] = tuple(frame[0])
+            rec["a_y"] = tuple(frame[1])
+            rec["a_z"] = tuple(frame[2])
+        else:
+            rec["type"] = 12
+            rec["dx"], rec["dy"] = semi[0], semi[1]
+            rec["l"] = 2 * semi[2]
+            rec["a_x"] = tuple(frame[0])
+            rec["a_y"] = tuple(frame[1])
+            rec["axis"] = tuple(frame[2])
+        for k in range(int(rng.integers(0, max_clips + 1))):
+            a = _unit(rng.standard_normal(3))
+            d = float(a @ c + rng.uniform(-0.5, 0.5) * ext)
+            cas = rec[f"cas{k + 1}"]
+            cas["axis"] = tuple(a)
+            cas["dotprod"] = d
+            cas["mode"] = int(rng.integers(1, 3))
+    return out

@@ -313,7 +313,12 @@ class Volume:
 
 
 class FBVolume:
-    """A volume given as FORBILD analytic shapes (mirrors volume.py:369-495)."""
+    """A volume given as FORBILD analytic shapes (mirrors volume.py:369-495).
+
+    ``shapes`` is an array of 156-byte FORBILD_Shape records (the reference's
+    layout; ``aprict_b200._structs.forbild_shape``). Later shapes override
+    earlier ones where they overlap (unless projected in additive mode).
+    """
 
     def __init__(self, shapes: np.ndarray) -> None:
         self.shapes = shapes
@@ -321,6 +326,29 @@ class FBVolume:
     def copy(self) -> FBVolume:
         """A copy of this phantom."""
         return FBVolume(self.shapes.copy())
+
+    def get_bbox(self) -> tuple[np.ndarray, np.ndarray]:
+        """(xyz_min, xyz_max) over all shapes (float32)."""
+        from .cb import forbild  # noqa: PLC0415
+
+        lo, hi = forbild.shape_bboxes(self.shapes)
+        return lo.min(axis=0).astype(np.float32), hi.max(axis=0).astype(np.float32)
+
+    @property
+    def minxyz_maxxyz(self) -> tuple[tuple[float, float, float], tuple[float, float, float]]:
+        """Bounding box ((minx,miny,minz),(maxx,maxy,maxz))."""
+        lo, hi = self.get_bbox()
+        return tuple(lo.tolist()), tuple(hi.tolist())  # type: ignore[return-value]
+
+    def prune_to_bbox(self, xyz_min: np.ndarray | tuple, xyz_max: np.ndarray | tuple) -> FBVolume:
+        """The shapes whose bounding box meets the given box (volume.py:454-495)."""
+        from .cb import forbild  # noqa: PLC0415
+
+        lo, hi = forbild.shape_bboxes(self.shapes)
+        bmin = np.asarray(xyz_min, dtype=np.float64)
+        bmax = np.asarray(xyz_max, dtype=np.float64)
+        keep = np.all(hi >= bmin, axis=1) & np.all(lo <= bmax, axis=1)
+        return FBVolume(self.shapes[keep])
 
     def superimpose_onto(self, vol: FBVolume) -> FBVolume:
         """This phantom's shapes drawn after (over) ``vol``'s."""

@@ -224,6 +224,71 @@ APRICT_API int aprict_b200_ramp_filter(const aprict_proj_desc *in, const float *
                                        int odd_taps_only, const float *weights_dev, int64_t w_stride_u,
                                        int64_t w_stride_v, float scale, aprict_stream_t stream);
 
+/* ---- Analytic (FORBILD) phantoms ---- */
+
+/* One clipping half-space (FORBILD_ClipAxisSpec, FORBILD_volumes.h:89-155):
+ * mode 0 = off, 1 = keep p.axis <= dotprod, 2 = keep p.axis > dotprod. */
+typedef struct {
+    aprict_fvec3 axis;
+    float dotprod;
+    uint8_t mode;
+    uint8_t pad_[3];
+} aprict_forbild_clip;
+
+/* One FORBILD shape, byte-identical to the reference's FORBILD_Shape
+ * (FORBILD_volumes.h:1395-1415; type map src/aprict/cuda/structs/FORBILD_volumes.py:517-534):
+ * 1 Box, 2-5 Cone/_x/_y/_z, 6-9 Cylinder/_x/_y/_z, 10 Ellipsoid,
+ * 11 Ellipsoid_free, 12 Ellipt_Cyl, 13 Sphere, 14-16 Ellipt_Cyl_x/_y/_z;
+ * 0 = no shape. 156 bytes. */
+typedef struct {
+    uint8_t type;
+    uint8_t pad_[3];
+    float rho;
+    aprict_forbild_clip cas1, cas2, cas3;
+    float x, y, z, dx, dy, dz, r, r1, r2, l;
+    aprict_fvec3 a_x, a_y, a_z, axis;
+} aprict_forbild_shape;
+
+/* A shape reduced (in FP64, on the host) to an affine map onto a canonical
+ * solid: local = M (p - c);
+ *   kind 1: |local| <= 1                       (ellipsoids, spheres)
+ *   kind 2: lx^2+ly^2 <= 1, |lz| <= h           (cylinders)
+ *   kind 3: lx^2+ly^2 <= (alpha+beta lz)^2, |lz| <= h   (cone frusta)
+ *   kind 4: |lx|,|ly|,|lz| <= 1                 (boxes)
+ * clipped by g_k(p) = clip[k].xyz . p - clip[k].w <= 0 for k < n_clip. */
+typedef struct {
+    int32_t kind;
+    int32_t n_clip;
+    double rho;
+    double c[3];
+    double M[9]; /* row-major */
+    double h, alpha, beta;
+    double clip[3][4];
+    double bb_half[3]; /* half extents of the world AABB about c */
+} aprict_quadric;
+
+/* Host function (no device work): compile n FORBILD shapes into
+ * aprict_quadric records. Null shapes (type 0) compile to kind 0. Returns
+ * APRICT_ERR_INVALID_ARGUMENT for an unknown type or degenerate parameters. */
+APRICT_API int aprict_b200_forbild_compile(const aprict_forbild_shape *shapes_host, int64_t n,
+                                           aprict_quadric *out_host);
+
+/* Analytic projection of compiled shapes, accumulated into projs
+ * (project_CB_FORBILD_shapes, CB_project_texture_chunked.cu:415-593):
+ *   mode 0: later shapes override earlier ones (the reference default,
+ *           exact_line_integral_prioritise_last, FORBILD_volumes.h:1889-1954);
+ *   mode 1: additive, sum rho * dt with dt the parametric chord on the
+ *           source->pixel segment (the reference's overlap_addition, :556-560,
+ *           which does not multiply by the segment length);
+ *   mode 2: additive line integral, sum rho * dt * |segment|.
+ * Entry/exit parameters are solved in FP64. Each CTA culls the shapes against
+ * its detector tile first. overflow_dev (optional) counts rays whose covered
+ * interval list overflowed in mode 0 (the reference's out_of_mem_count). */
+APRICT_API int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, const aprict_proj_desc *projs,
+                                           float *projs_dev, const aprict_quadric *shapes_dev, int64_t n_shapes,
+                                           float multiply_before_adding, uint32_t ssu, uint32_t ssv, int mode,
+                                           uint32_t *overflow_dev, uint32_t *status_dev, aprict_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -402,3 +402,275 @@ void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, cons
     free(priv);
     free(tmp);
 }
+
+/* ---- FORBILD analytic shapes (FORBILD_volumes.h), FP64 ----
+ * Each shape type is intersected in its own natural coordinates as the
+ * reference structures it: spheres and ellipsoids by a quadratic in the
+ * (scaled) frame, cylinders as an axial slab with a radial quadratic, boxes as
+ * three slabs, cone frusta as an axial slab with a quadratic for the linearly
+ * varying radius; clip planes first (FORBILD_volumes.h:1723-1811). All
+ * intervals are parameters along the segment, clamped to [0, 1]. */
+
+typedef struct {
+    double lo, hi;
+} iv_t;
+
+static void iv_and_lin(iv_t *I, double a, double b) { /* keep a + b t <= 0 */
+    if (b == 0.0) {
+        if (a > 0.0) I->hi = I->lo - 1.0;
+        return;
+    }
+    const double t = -a / b;
+    if (b > 0.0) {
+        if (t < I->hi) I->hi = t;
+    } else if (t > I->lo) {
+        I->lo = t;
+    }
+}
+
+static void iv_and_slab(iv_t *I, double p, double d, double h) { /* keep |p + t d| <= h */
+    iv_and_lin(I, p - h, d);
+    iv_and_lin(I, -p - h, -d);
+}
+
+/* keep A t^2 + B t + C <= 0 (a convex set for A > 0; for A < 0 the caller's
+ * slab keeps one nappe) */
+static void iv_and_quad(iv_t *I, double A, double B, double C) {
+    if (A == 0.0) {
+        iv_and_lin(I, C, B);
+        return;
+    }
+    const double disc = B * B - 4.0 * A * C;
+    if (A > 0.0) {
+        if (!(disc > 0.0)) {
+            I->hi = I->lo - 1.0;
+            return;
+        }
+        const double sq = sqrt(disc);
+        const double t0 = (-B - sq) / (2.0 * A), t1 = (-B + sq) / (2.0 * A);
+        if (t0 > I->lo) I->lo = t0;
+        if (t1 < I->hi) I->hi = t1;
+        return;
+    }
+    if (!(disc > 0.0)) return; /* A < 0, no real roots: q < 0 everywhere */
+    const double sq = sqrt(disc);
+    double t0 = (-B + sq) / (2.0 * A), t1 = (-B - sq) / (2.0 * A);
+    if (t0 > t1) {
+        const double x = t0;
+        t0 = t1;
+        t1 = x;
+    }
+    /* solution: (-inf, t0] U [t1, inf); within [lo, hi] keep the part that exists */
+    const int a_ok = I->lo < fmin(I->hi, t0), b_ok = fmax(I->lo, t1) < I->hi;
+    if (a_ok && !b_ok) I->hi = fmin(I->hi, t0);
+    if (b_ok && !a_ok) I->lo = fmax(I->lo, t1);
+    if (!a_ok && !b_ok) I->hi = I->lo - 1.0;
+}
+
+static void unit3(ao_fvec3 v, double o[3]) {
+    const double n = sqrt((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    o[0] = v.x / n;
+    o[1] = v.y / n;
+    o[2] = v.z / n;
+}
+static double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* cylinder-like solid: local coords (x, y) scaled to the unit disc, z axial */
+static void iv_ecyl(iv_t *I, const double p[3], const double d[3], const double ax[3], double sx, const double ay[3],
+                    double sy, const double az[3], double h) {
+    const double px = dot3(p, ax) / sx, py = dot3(p, ay) / sy, pz = dot3(p, az);
+    const double dx = dot3(d, ax) / sx, dy = dot3(d, ay) / sy, dz = dot3(d, az);
+    iv_and_slab(I, pz, dz, h);
+    iv_and_quad(I, dx * dx + dy * dy, 2.0 * (px * dx + py * dy), px * px + py * py - 1.0);
+}
+
+static void perp2(const double a[3], double e1[3], double e2[3]) {
+    const double t[3] = {fabs(a[0]) < 0.9 ? 1.0 : 0.0, fabs(a[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    double c[3] = {a[1] * t[2] - a[2] * t[1], a[2] * t[0] - a[0] * t[2], a[0] * t[1] - a[1] * t[0]};
+    const double n = sqrt(dot3(c, c));
+    e1[0] = c[0] / n;
+    e1[1] = c[1] / n;
+    e1[2] = c[2] / n;
+    e2[0] = a[1] * e1[2] - a[2] * e1[1];
+    e2[1] = a[2] * e1[0] - a[0] * e1[2];
+    e2[2] = a[0] * e1[1] - a[1] * e1[0];
+}
+
+int ao_forbild_interval(const double v1[3], const double v2[3], const ao_forbild_shape *s, double out2[2]) {
+    iv_t I = {0.0, 1.0};
+    const double d[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+    out2[0] = out2[1] = 0.0;
+    if (s->type == 0) return 0;
+    for (int k = 0; k < 3; ++k) {
+        const ao_clip *c = &s->cas[k];
+        if (c->mode == 0) continue;
+        const double a[3] = {c->axis.x, c->axis.y, c->axis.z};
+        const double g0 = dot3(a, v1) - c->dotprod, gd = dot3(a, d);
+        if (c->mode == 1)
+            iv_and_lin(&I, g0, gd);
+        else
+            iv_and_lin(&I, -g0, -gd);
+    }
+    if (!(I.lo < I.hi)) return 0;
+    const double p[3] = {v1[0] - s->x, v1[1] - s->y, v1[2] - s->z};
+    const double ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0}, ez[3] = {0, 0, 1};
+    double ax[3], ay[3], az[3];
+    switch (s->type) {
+        case 13: /* sphere */
+            iv_and_quad(&I, dot3(d, d), 2.0 * dot3(p, d), dot3(p, p) - (double)s->r * s->r);
+            break;
+        case 10: { /* axis-aligned ellipsoid: scale each coordinate */
+            const double sc[3] = {s->dx, s->dy, s->dz};
+            double pp[3], dd[3];
+            for (int i = 0; i < 3; ++i) {
+                pp[i] = p[i] / sc[i];
+                dd[i] = d[i] / sc[i];
+            }
+            iv_and_quad(&I, dot3(dd, dd), 2.0 * dot3(pp, dd), dot3(pp, pp) - 1.0);
+            break;
+        }
+        case 11: { /* free ellipsoid */
+            unit3(s->a_x, ax);
+            unit3(s->a_y, ay);
+            unit3(s->a_z, az);
+            const double pp[3] = {dot3(p, ax) / s->dx, dot3(p, ay) / s->dy, dot3(p, az) / s->dz};
+            const double dd[3] = {dot3(d, ax) / s->dx, dot3(d, ay) / s->dy, dot3(d, az) / s->dz};
+            iv_and_quad(&I, dot3(dd, dd), 2.0 * dot3(pp, dd), dot3(pp, pp) - 1.0);
+            break;
+        }
+        case 12:
+            unit3(s->a_x, ax);
+            unit3(s->a_y, ay);
+            unit3(s->axis, az);
+            iv_ecyl(&I, p, d, ax, s->dx, ay, s->dy, az, 0.5 * s->l);
+            break;
+        case 14: iv_ecyl(&I, p, d, ey, s->dy, ez, s->dz, ex, 0.5 * s->l); break;
+        case 15: iv_ecyl(&I, p, d, ex, s->dx, ez, s->dz, ey, 0.5 * s->l); break;
+        case 16: iv_ecyl(&I, p, d, ex, s->dx, ey, s->dy, ez, 0.5 * s->l); break;
+        case 6:
+        case 7:
+        case 8:
+        case 9: { /* circular cylinder: radial distance from the axis */
+            double a[3];
+            if (s->type == 6)
+                unit3(s->axis, a);
+            else
+                memcpy(a, s->type == 7 ? ex : (s->type == 8 ? ey : ez), sizeof(a));
+            const double pz = dot3(p, a), dz = dot3(d, a);
+            iv_and_slab(&I, pz, dz, 0.5 * s->l);
+            const double pr[3] = {p[0] - pz * a[0], p[1] - pz * a[1], p[2] - pz * a[2]};
+            const double dr[3] = {d[0] - dz * a[0], d[1] - dz * a[1], d[2] - dz * a[2]};
+            iv_and_quad(&I, dot3(dr, dr), 2.0 * dot3(pr, dr), dot3(pr, pr) - (double)s->r * s->r);
+            break;
+        }
+        case 2:
+        case 3:
+        case 4:
+        case 5: { /* cone frustum, radius r1 at -l/2 .. r2 at +l/2 */
+            double a[3], e1[3], e2[3];
+            if (s->type == 2)
+                unit3(s->axis, a);
+            else
+                memcpy(a, s->type == 3 ? ex : (s->type == 4 ? ey : ez), sizeof(a));
+            perp2(a, e1, e2);
+            const double h = 0.5 * s->l;
+            const double pz = dot3(p, a), dz = dot3(d, a);
+            iv_and_slab(&I, pz, dz, h);
+            if (!(I.lo < I.hi)) return 0;
+            const double px = dot3(p, e1), py = dot3(p, e2), dx = dot3(d, e1), dy = dot3(d, e2);
+            const double al = 0.5 * ((double)s->r1 + s->r2), be = ((double)s->r2 - s->r1) / s->l;
+            const double ra = al + be * pz, rb = be * dz;
+            iv_and_quad(&I, dx * dx + dy * dy - rb * rb, 2.0 * (px * dx + py * dy - ra * rb), px * px + py * py - ra * ra);
+            break;
+        }
+        case 1: /* box of full side lengths */
+            iv_and_slab(&I, p[0], d[0], 0.5 * s->dx);
+            iv_and_slab(&I, p[1], d[1], 0.5 * s->dy);
+            iv_and_slab(&I, p[2], d[2], 0.5 * s->dz);
+            break;
+        default: return 0;
+    }
+    if (!(I.lo < I.hi)) return 0;
+    out2[0] = I.lo;
+    out2[1] = I.hi;
+    return 1;
+}
+
+static int cmp_double(const void *a, const void *b) {
+    const double x = *(const double *)a, y = *(const double *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+void ao_project_forbild(const ao_proj_spec *specs, int n_views, int nu, int nv, const ao_forbild_shape *shapes,
+                        int n_shapes, double mba, int mode, int ssu, int ssv, double *out, int nthreads) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+    {
+        double *lo = (double *)malloc(sizeof(double) * (size_t)(n_shapes + 1));
+        double *hi = (double *)malloc(sizeof(double) * (size_t)(n_shapes + 1));
+        double *rho = (double *)malloc(sizeof(double) * (size_t)(n_shapes + 1));
+        double *ev = (double *)malloc(sizeof(double) * (size_t)(2 * n_shapes + 2));
+#pragma omp for collapse(2) schedule(dynamic, 4)
+        for (int m = 0; m < n_views; ++m) {
+            for (int iu = 0; iu < nu; ++iu) {
+                const ao_proj_spec *sp = &specs[m];
+                const double s[3] = {sp->source_pos.x, sp->source_pos.y, sp->source_pos.z};
+                for (int iv = 0; iv < nv; ++iv) {
+                    double tot = 0.0;
+                    for (int ku = 0; ku < ssu; ++ku) {
+                        double accu = 0.0;
+                        for (int kv = 0; kv < ssv; ++kv) {
+                            const d3 pp = pixel_pos(sp, iu - 0.5 + (ku + 0.5) / ssu, iv - 0.5 + (kv + 0.5) / ssv);
+                            const double e[3] = {pp.x, pp.y, pp.z};
+                            const double len = sqrt((e[0] - s[0]) * (e[0] - s[0]) + (e[1] - s[1]) * (e[1] - s[1]) +
+                                                    (e[2] - s[2]) * (e[2] - s[2]));
+                            int k = 0;
+                            for (int j = 0; j < n_shapes; ++j) {
+                                double r[2];
+                                if (ao_forbild_interval(s, e, &shapes[j], r)) {
+                                    lo[k] = r[0];
+                                    hi[k] = r[1];
+                                    rho[k] = shapes[j].rho;
+                                    ++k;
+                                }
+                            }
+                            double val = 0.0;
+                            if (mode != 0) {
+                                for (int i = 0; i < k; ++i) val += rho[i] * (hi[i] - lo[i]);
+                                if (mode == 2) val *= len;
+                            } else if (k > 0) {
+                                /* elementary segments between all endpoints; each is
+                                 * charged to the last shape covering its midpoint */
+                                int ne = 0;
+                                for (int i = 0; i < k; ++i) {
+                                    ev[ne++] = lo[i];
+                                    ev[ne++] = hi[i];
+                                }
+                                qsort(ev, (size_t)ne, sizeof(double), cmp_double);
+                                for (int q = 0; q + 1 < ne; ++q) {
+                                    const double a = ev[q], b = ev[q + 1];
+                                    if (!(b > a)) continue;
+                                    const double mid = 0.5 * (a + b);
+                                    for (int i = k - 1; i >= 0; --i) {
+                                        if (lo[i] <= mid && mid <= hi[i]) {
+                                            val += rho[i] * (b - a);
+                                            break;
+                                        }
+                                    }
+                                }
+                                val *= len;
+                            }
+                            accu += val * mba;
+                        }
+                        tot += accu / ssv;
+                    }
+                    out[((int64_t)m * nu + iu) * nv + iv] += tot / ssu;
+                }
+            }
+        }
+        free(lo);
+        free(hi);
+        free(rho);
+        free(ev);
+    }
+}

@@ -49,4 +49,27 @@ void ao_backproject_transpose(const ao_proj_spec *specs, int n_views, int nu, in
 void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
                     const ao_grid *g, const double *mult, const ao_bp_cfg *cfg, double *vol, int nthreads);
 
+/* Reference layout of FORBILD_Shape (FORBILD_volumes.h:1395-1415), 156 bytes. */
+typedef struct {
+    ao_fvec3 axis;
+    float dotprod;
+    uint8_t mode, pad_[3];
+} ao_clip;
+typedef struct {
+    uint8_t type, pad_[3];
+    float rho;
+    ao_clip cas[3];
+    float x, y, z, dx, dy, dz, r, r1, r2, l;
+    ao_fvec3 a_x, a_y, a_z, axis;
+} ao_forbild_shape;
+
+/* out[m,iu,iv] += mba * analytic projection of the shapes (FP64):
+ * mode 0 later shapes win (x |segment|), 1 sum rho*dt, 2 sum rho*dt*|segment|
+ * (project_CB_FORBILD_shapes, CB_project_texture_chunked.cu:415-593). */
+void ao_project_forbild(const ao_proj_spec *specs, int n_views, int nu, int nv, const ao_forbild_shape *shapes,
+                        int n_shapes, double mba, int mode, int ssu, int ssv, double *out, int nthreads);
+
+/* Interval [t0,t1] of the segment v1->v2 with one shape (after clipping), FP64. */
+int ao_forbild_interval(const double v1[3], const double v2[3], const ao_forbild_shape *s, double out2[2]);
+
 #endif

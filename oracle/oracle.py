@@ -303,3 +303,72 @@ def ref_backproject(
         msg = f"reference backprojector accessed outside the volume {oob} times"
         raise RuntimeError(msg)
     return vol
+
+
+# --------------------------------------------------------------------- FORBILD shapes
+def project_forbild(
+    specs: np.ndarray,
+    shapes: np.ndarray,
+    *,
+    mba: float = 1.0,
+    mode: int = 0,
+    ssu: int = 1,
+    ssv: int = 1,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """FP64 analytic projection of FORBILD shapes; mode 0 later-wins, 1 sum rho dt, 2 sum rho dt |seg|."""
+    lib = _load(ORACLE_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    sh = np.ascontiguousarray(shapes.reshape(-1))
+    out = np.zeros((m, nu, nv), dtype=np.float64)
+    lib.ao_project_forbild(
+        _p(s), m, nu, nv, _p(sh), len(sh), ctypes.c_double(mba), mode, ssu, ssv, _p(out), nthreads or nthreads_default()
+    )
+    return out
+
+
+def forbild_interval(v1: np.ndarray, v2: np.ndarray, shape: np.ndarray) -> tuple[float, float] | None:
+    """FP64 interval of segment v1->v2 with one shape (None if empty)."""
+    lib = _load(ORACLE_SO)
+    a = np.asarray(v1, np.float64)
+    b = np.asarray(v2, np.float64)
+    o = np.zeros(2)
+    sh = np.ascontiguousarray(shape.reshape(1))
+    ok = lib.ao_forbild_interval(_p(a), _p(b), _p(sh), _p(o))
+    return (float(o[0]), float(o[1])) if ok else None
+
+
+def ref_project_forbild(
+    specs: np.ndarray,
+    shapes: np.ndarray,
+    *,
+    mba: float = 1.0,
+    overlap_addition: bool = False,
+    ssu: int = 1,
+    ssv: int = 1,
+    nthreads: int | None = None,
+) -> tuple[np.ndarray, int]:
+    """The reference's FORBILD projection body run on the CPU: (out float32, overflow count)."""
+    lib = _load(REF_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    sh = np.ascontiguousarray(shapes.reshape(-1))
+    out = np.zeros((m, nu, nv), dtype=np.float32)
+    ovf = ctypes.c_uint(0)
+    lib.ref_project_forbild(
+        _p(s), m, nu, nv, _p(sh), len(sh), ctypes.c_float(mba), int(overlap_addition), ssu, ssv, _p(out),
+        ctypes.byref(ovf), nthreads or nthreads_default(),
+    )
+    return out, int(ovf.value)
+
+
+def ref_forbild_interval(v1: np.ndarray, v2: np.ndarray, shape: np.ndarray) -> tuple[float, float]:
+    """The reference's FORBILD_clip_line_segment(FORBILD_Shape) on the CPU (FP32)."""
+    lib = _load(REF_SO)
+    a = np.asarray(v1, np.float32)
+    b = np.asarray(v2, np.float32)
+    o = np.zeros(2, np.float32)
+    sh = np.ascontiguousarray(shape.reshape(1))
+    lib.ref_forbild_interval(_p(a), _p(b), _p(sh), _p(o))
+    return float(o[0]), float(o[1])
