@@ -23,6 +23,8 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "aprict_b200_last_error": (_c_char_p, []),
     "aprict_b200_version": (_c_char_p, []),
     "aprict_b200_struct_size": (ctypes.c_size_t, [_c_char_p]),
+    "aprict_b200_set_tuning": (_c_int, [_c_int, _c_int]),
+    "aprict_b200_get_tuning": (_c_int, [_c_int]),
     "aprict_b200_project_siddon": (
         _c_int,
         [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p],

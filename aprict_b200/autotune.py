@@ -1,0 +1,119 @@
+"""Launch-shape autotuner.
+
+Times a few candidate launch shapes of the forward projector (detector tile
+height) and the backprojector (voxels per thread, size of the brick-ordered
+wave) on the caller's own problem with CUDA events, keeps the fastest, and
+applies it through ``aprict_b200_set_tuning``. Results never depend on these
+knobs; only speed does. Choices are cached per problem signature (in memory,
+and optionally in a JSON file).
+"""
+
+from __future__ import annotations
+
+import json
+import pathlib
+import threading
+
+import torch
+
+from . import _lib
+from .cb import flatpanel as fp
+from .volume import Volume
+
+KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE = 0, 1, 2
+FP_TILE_V = (8, 16, 32)
+BP_XB = (2, 4)
+BP_WAVE = (2, 3, 4, 6)
+
+_cache: dict[str, dict] = {}
+_lock = threading.Lock()
+
+
+def _set(key: int, value: int) -> None:
+    _lib.check(_lib.lib().aprict_b200_set_tuning(key, int(value)), "set_tuning")
+
+
+def current() -> dict:
+    """The knobs in effect (0 = built-in default)."""
+    lib = _lib.lib()
+    return {"fp_tile_v": lib.aprict_b200_get_tuning(0), "bp_xb": lib.aprict_b200_get_tuning(1), "bp_wave": lib.aprict_b200_get_tuning(2)}
+
+
+def apply(choice: dict) -> None:
+    """Apply a choice returned by :func:`tune`."""
+    _set(KEY_FP_TILE_V, choice.get("fp_tile_v", 0))
+    _set(KEY_BP_XB, choice.get("bp_xb", 0))
+    _set(KEY_BP_WAVE, choice.get("bp_wave", 0))
+
+
+def _time(fn, reps: int = 3) -> float:
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def signature(projs: fp.ProjectionSet, volume: Volume, cfg_bp: fp.ConfigBackproject | None) -> str:
+    """Cache key: data shapes, volume order and the backprojection settings."""
+    c = None if cfg_bp is None else cfg_bp.contents.tobytes().hex()
+    return json.dumps([list(projs.data.shape), list(volume.shape), volume.order, c])
+
+
+def tune(
+    projs: fp.ProjectionSet,
+    volume: Volume,
+    *,
+    cfg_bp: fp.ConfigBackproject | None = None,
+    multiplier: Volume | None = None,
+    cache_file: str | pathlib.Path | None = None,
+    reps: int = 2,
+) -> dict:
+    """Choose and apply the fastest launch shapes for this problem; returns the choice.
+
+    Runs a handful of projections into a scratch copy of ``projs`` and
+    backprojections into a scratch copy of ``volume``; the inputs are not modified.
+    """
+    sig = signature(projs, volume, cfg_bp)
+    disk: dict = {}
+    if cache_file is not None and pathlib.Path(cache_file).exists():
+        disk = json.loads(pathlib.Path(cache_file).read_text())
+    with _lock:
+        if sig in _cache:
+            apply(_cache[sig])
+            return dict(_cache[sig])
+        if sig in disk:
+            _cache[sig] = disk[sig]
+            apply(disk[sig])
+            return dict(disk[sig])
+    choice: dict = {}
+    scratch_p = projs.zeroed_copy()
+    cfg_fp = fp.ConfigProject()
+    times = {}
+    for tv in FP_TILE_V:
+        _set(KEY_FP_TILE_V, tv)
+        times[tv] = _time(lambda: fp.project(cfg_fp, volume, scratch_p), reps)
+    choice["fp_tile_v"] = min(times, key=times.get)
+    choice["fp_ms"] = round(times[choice["fp_tile_v"]], 4)
+    if cfg_bp is not None:
+        scratch_v = volume.zeroed_copy()
+        best = None
+        for xb in BP_XB:
+            for wave in BP_WAVE:
+                _set(KEY_BP_XB, xb)
+                _set(KEY_BP_WAVE, wave)
+                t = _time(lambda: fp.backproject(cfg_bp, scratch_v, projs, summand_multiplier=multiplier), reps)
+                if best is None or t < best[0]:
+                    best = (t, xb, wave)
+        choice["bp_xb"], choice["bp_wave"], choice["bp_ms"] = best[1], best[2], round(best[0], 4)
+    apply(choice)
+    with _lock:
+        _cache[sig] = choice
+        if cache_file is not None:
+            disk[sig] = choice
+            pathlib.Path(cache_file).write_text(json.dumps(disk, indent=1))
+    return dict(choice)

@@ -27,7 +27,6 @@ namespace {
 
 constexpr int kThreads = 256;  // 32 (fast axis) x 8 (middle axis)
 constexpr int kChunk = 128;    // views per shared-memory chunk
-constexpr int kXB = 4;         // voxels per thread along the slowest axis
 
 struct BPParams {
     const aprict_proj_spec *specs;
@@ -65,31 +64,29 @@ struct BPParams {
 // again in FP64 from the voxel's FP64 position.
 constexpr float kRefine = 2e-3f;
 
+// FP64 position of a voxel (centre + sub-sample offset) relative to the
+// volume centre, from its integer indices: exact in double.
 struct VoxRef {
-    int ix, iy, iz;    // voxel indices
-    float fx, fy, fz;  // sub-voxel offsets in voxels (0 without supersampling)
+    double x, y, z;
 };
 
-// Out of line: only the rare near-tie path pays for its FP64 registers.
-__device__ __noinline__ float refine_nearest(const BPParams &P, const float *pvw, int view, VoxRef r) {
-    const ab_d3 x{P.cornerd[0] + ((double)r.ix + 0.5 + (double)r.fx) * P.vwd,
-                  P.cornerd[1] + ((double)r.iy + 0.5 + (double)r.fy) * P.vwd,
-                  P.cornerd[2] + ((double)r.iz + 0.5 + (double)r.fz) * P.vwd};
-    double du, dv;
-    const aprict_proj_spec sp = P.specs[view];
-    ab_project_point_d(sp, x, du, dv);
+__device__ __forceinline__ float refine_nearest(const BPParams &P, const float *pvw, const ab_bpview_d &c,
+                                                const VoxRef &r) {
+    const double D = fma(c.den[0], r.x, fma(c.den[1], r.y, fma(c.den[2], r.z, c.den[3])));
+    const double du = fma(c.nu[0], r.x, fma(c.nu[1], r.y, fma(c.nu[2], r.z, c.nu[3]))) / D;
+    const double dv = fma(c.nv[0], r.x, fma(c.nv[1], r.y, fma(c.nv[2], r.z, c.nv[3]))) / D;
     const double gu = floor(du + 0.5), gv = floor(dv + 0.5);
     if (!(gu >= 0.0 && gu < (double)P.nu && gv >= 0.0 && gv < (double)P.nv)) return 0.f;
     return __ldg(pvw + ((int)gu * P.su + (int)gv * P.sv));
 }
 
-__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pvw, int view, float fu, float fv,
-                                               const VoxRef &r) {
+__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pvw, const ab_bpview_d &c,
+                                               float fu, float fv, const VoxRef &r) {
     const float gu = fu + 0.5f, gv = fv + 0.5f;
     const float lu = floorf(gu), lv = floorf(gv);
     // |frac - 1/2| <= 1/2 - kRefine on both axes, written so that NaN fails
     if (!(fabsf(gu - lu - 0.5f) <= 0.5f - kRefine && fabsf(gv - lv - 0.5f) <= 0.5f - kRefine))
-        return refine_nearest(P, pvw, view, r);
+        return refine_nearest(P, pvw, c, r);
     // float -> int saturates, so out-of-range values fail the unsigned test
     const int iu = (int)lu, iv = (int)lv;
     if ((unsigned)iu >= P.nu || (unsigned)iv >= P.nv) return 0.f;
@@ -140,9 +137,14 @@ __device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, flo
 // RAYCAST: fast mode with direct-raycast weights (:512-646, preset 0).
 // BILIN: bilinear instead of nearest detector sampling.
 // ORD: 0 = C order (fastest axis z, slowest x), 1 = F order (fastest x).
-template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
-__global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
+// XB: voxels per thread along the slowest axis (4: more reuse of each view's
+// coefficients, 2: fewer registers and more resident warps).
+template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
+__global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(BPParams P) {
+    constexpr int kXB = XB;
+    constexpr bool kNear = !EXACT && !BILIN;
     __shared__ ab_bpview sv[kChunk];
+    __shared__ ab_bpview_d svd[kNear ? kChunk : 1];
     __shared__ ab_bpview_exact sx[EXACT ? kChunk : 1];
 
     // Brick-ordered block coordinates (uniform per CTA).
@@ -196,7 +198,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
 #pragma unroll
     for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
 
-    const ab_d3 c0d{(double)P.c0[0], (double)P.c0[1], (double)P.c0[2]};
+    // Volume centre in FP64 (exact: corner and voxwid are floats, n an integer).
+    const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
+                    P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
     const bool needZ = P.pL != 0 || P.pV != 0;
     const int n_sub = P.ssx * P.ssy * P.ssz;
@@ -213,7 +217,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
                     __syncthreads();
                     for (int t = threadIdx.x; t < cn; t += kThreads) {
                         const aprict_proj_spec sp = P.specs[v0 + t];
-                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t]) && P.status)
+                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t], kNear ? &svd[t] : nullptr) && P.status)
                             atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
                     }
@@ -328,8 +332,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
                                         id[a0] = i0;
                                         id[a1] = i1;
                                         id[a2] = i2b + k;
-                                        const VoxRef vr{id[0], id[1], id[2], fsub[0], fsub[1], fsub[2]};
-                                        pv = fetch_nearest(P, pvw, view, fu, fv, vr);
+                                        const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                        ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                        ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
+                                        pv = fetch_nearest(P, pvw, svd[kNear ? t : 0], fu, fv, vr);
                                     }
                                 }
                                 s = pv * w;
@@ -358,20 +364,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_backproject(BPParams P) {
     }
 }
 
-template <int ORD>
+template <int ORD, int XB>
 void launch_bp(const BPParams &P, const aprict_backproject_config *cfg, bool lin, unsigned grid, cudaStream_t st) {
     if (cfg->exact) {
-        k_backproject<ORD, true, false, false><<<grid, kThreads, 0, st>>>(P);
+        k_backproject<ORD, true, false, false, XB><<<grid, kThreads, 0, st>>>(P);
     } else if (cfg->approx_mode_direct_raycast) {
         if (lin)
-            k_backproject<ORD, false, true, true><<<grid, kThreads, 0, st>>>(P);
+            k_backproject<ORD, false, true, true, XB><<<grid, kThreads, 0, st>>>(P);
         else
-            k_backproject<ORD, false, true, false><<<grid, kThreads, 0, st>>>(P);
+            k_backproject<ORD, false, true, false, XB><<<grid, kThreads, 0, st>>>(P);
     } else {
         if (lin)
-            k_backproject<ORD, false, false, true><<<grid, kThreads, 0, st>>>(P);
+            k_backproject<ORD, false, false, true, XB><<<grid, kThreads, 0, st>>>(P);
         else
-            k_backproject<ORD, false, false, false><<<grid, kThreads, 0, st>>>(P);
+            k_backproject<ORD, false, false, false, XB><<<grid, kThreads, 0, st>>>(P);
     }
 }
 
@@ -446,6 +452,8 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.ssz = (int)cfg->ssz;
     P.status = status_dev;
 
+    const int xb = ab_tuning_get(AB_TUNE_BP_XB) == 2 ? 2 : 4;
+    const int kXB = xb;
     const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
     P.gb[0] = (n0 + 31) / 32;
     P.gb[1] = (n1 + 7) / 8;
@@ -459,7 +467,8 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
-    const double target = 3.0 * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
+    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : 3;
+    const double target = (double)wave * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
     int sb1 = (int)floor(sqrt(target * kXB / 8.0) + 0.5);
     sb1 = sb1 < 1 ? 1 : (sb1 > P.gb[1] ? P.gb[1] : sb1);
     int sb2 = (int)floor(target / sb1 + 0.5);
@@ -472,9 +481,16 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     if (grid > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const bool lin = cfg->approx_mode_linear_interpolate != 0;
-    if (vd->order == 0)
-        launch_bp<0>(P, cfg, lin, (unsigned)grid, st);
-    else
-        launch_bp<1>(P, cfg, lin, (unsigned)grid, st);
+    if (xb == 4) {
+        if (vd->order == 0)
+            launch_bp<0, 4>(P, cfg, lin, (unsigned)grid, st);
+        else
+            launch_bp<1, 4>(P, cfg, lin, (unsigned)grid, st);
+    } else {
+        if (vd->order == 0)
+            launch_bp<0, 2>(P, cfg, lin, (unsigned)grid, st);
+        else
+            launch_bp<1, 2>(P, cfg, lin, (unsigned)grid, st);
+    }
     return ab_cuda_check(cudaGetLastError(), "backproject launch");
 }

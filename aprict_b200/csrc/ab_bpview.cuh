@@ -35,6 +35,12 @@ struct ab_bpview {
     float cu0, cv0, tap_ru, tap_rv;
 };
 
+// The same three linear forms in FP64 (coefficients before rounding), used to
+// settle nearest-pixel choices that the FP32 forms cannot resolve.
+struct ab_bpview_d {
+    double nu[4], nv[4], den[4];
+};
+
 // Exact-mode extras: ray origin and per-pixel direction in world units,
 // relative to the volume centre.
 struct ab_bpview_exact {
@@ -44,7 +50,8 @@ struct ab_bpview_exact {
     float4 v;   // det_v
 };
 
-AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, float sep, ab_bpview &o) {
+AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, float sep, ab_bpview &o,
+                            ab_bpview_d *od = nullptr) {
     const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
     const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);
     const ab_d3 n = ab_cross(U, V);
@@ -57,6 +64,7 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
               ab_finite3(U) && ab_finite3(V);
     if (!ok) {
         o = ab_bpview{};
+        if (od) *od = ab_bpview_d{};
         return false;
     }
     const double hu = ((double)sp.nu - 1.0) * 0.5, hv = ((double)sp.nv - 1.0) * 0.5;
@@ -64,6 +72,10 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     const ab_d3 Au = (U * Dn - n * ab_dot(U, Ps)) * (1.0 / uu) + n * hu;
     const ab_d3 Av = (V * Dn - n * ab_dot(V, Ps)) * (1.0 / vv) + n * hv;
     const ab_d3 Lh = Ps * (1.0 / Lnorm);
+    if (od) {
+        *od = ab_bpview_d{{Au.x, Au.y, Au.z, ab_dot(Au, c0s)}, {Av.x, Av.y, Av.z, ab_dot(Av, c0s)},
+                          {n.x, n.y, n.z, ab_dot(n, c0s)}};
+    }
     o.nu = make_float4((float)Au.x, (float)Au.y, (float)Au.z, (float)ab_dot(Au, c0s));
     o.nv = make_float4((float)Av.x, (float)Av.y, (float)Av.z, (float)ab_dot(Av, c0s));
     o.den = make_float4((float)n.x, (float)n.y, (float)n.z, (float)ab_dot(n, c0s));

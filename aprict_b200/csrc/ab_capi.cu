@@ -13,6 +13,9 @@ static_assert(sizeof(aprict_project_config) == 16, "project_config layout");
 static_assert(sizeof(aprict_backproject_config) == 76, "backproject_config layout");
 
 static thread_local char g_last_error[512] = "";
+static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0};
+
+int ab_tuning_get(int key) { return key >= 0 && key < AB_TUNE_COUNT ? __atomic_load_n(&g_tuning[key], __ATOMIC_RELAXED) : 0; }
 
 void ab_set_error(const char *fmt, ...) {
     va_list ap;
@@ -89,6 +92,21 @@ const char *aprict_b200_status_string(int status) {
 const char *aprict_b200_last_error(void) { return g_last_error; }
 
 const char *aprict_b200_version(void) { return "0.1.0"; }
+
+int aprict_b200_set_tuning(int key, int value) {
+    if (key < 0 || key >= AB_TUNE_COUNT) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "unknown tuning key %d", key);
+    bool ok;
+    switch (key) {
+        case AB_TUNE_FP_TILE_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
+        case AB_TUNE_BP_XB: ok = value == 0 || value == 2 || value == 4; break;
+        default: ok = value >= 0 && value <= 16; break;
+    }
+    if (!ok) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "tuning value %d not allowed for key %d", value, key);
+    __atomic_store_n(&g_tuning[key], value, __ATOMIC_RELAXED);
+    return APRICT_OK;
+}
+
+int aprict_b200_get_tuning(int key) { return ab_tuning_get(key); }
 
 size_t aprict_b200_struct_size(const char *name) {
     if (name == nullptr) return 0;

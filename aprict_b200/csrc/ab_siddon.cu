@@ -8,8 +8,7 @@
 // B200 layout: a CTA covers a 2-D detector tile of one view and each warp a
 // 4 (u) x 8 (v) pixel patch, so the rays of a warp are spatially coherent and
 // their voxel gathers hit the same L1 lines; 8 consecutive v per row make the
-// output access one 32-byte sector. CTAs are ordered view-major so the CTAs
-// resident at one time cover 1-2 views and share the volume working set in L2.
+// output access one 32-byte sector.
 #include <cuda_runtime.h>
 
 #include "ab_common.cuh"
@@ -29,6 +28,8 @@ struct TileMap {
 TileMap make_tiles(uint32_t nu, uint32_t nv) {
     TileMap t;
     t.tile_v = nv >= 16 ? 16 : (nv >= 8 ? 8 : 1);
+    const int want = ab_tuning_get(AB_TUNE_FP_TILE_V);  // autotuner override: 8, 16 or 32
+    if ((want == 8 || want == 16 || want == 32) && nv >= 8) t.tile_v = want;
     t.tile_u = kThreads / t.tile_v;
     t.ntu = (int)((nu + t.tile_u - 1) / t.tile_u);
     t.ntv = (int)((nv + t.tile_v - 1) / t.tile_v);

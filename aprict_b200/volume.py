@@ -301,6 +301,35 @@ class Volume:
             self.fill(0.0)
         return self
 
+    @classmethod
+    def from_tensor(
+        cls,
+        t: torch.Tensor,
+        *,
+        voxwid: float,
+        pos_c: np.ndarray | tuple[float, float, float] = (0.0, 0.0, 0.0),
+    ) -> Volume:
+        """Wrap a float32 CUDA tensor of shape (X,Y,Z) without copying (C- or F-contiguous)."""
+        if t.dim() != 3 or t.dtype != torch.float32 or not t.is_cuda:
+            msg = "from_tensor needs a 3-D float32 CUDA tensor"
+            raise ValueError(msg)
+        X, Y, Z = t.shape  # noqa: N806
+        if t.stride() == (Y * Z, Z, 1):
+            order = "C"
+        elif t.stride() == (1, X, X * Y):
+            order = "F"
+        else:
+            msg = "from_tensor needs a C- or F-contiguous tensor"
+            raise ValueError(msg)
+        self = cls.__new__(cls)
+        self._shape = (int(X), int(Y), int(Z))
+        self._dtype = np.dtype(np.float32)
+        self._order = order  # type: ignore[assignment]
+        self._voxwid = float(voxwid)
+        self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
+        self._data = t
+        return self
+
     def zeroed_copy(self) -> Volume:
         """A zero-filled volume with this geometry."""
         return Volume.zeros(self._shape, voxwid=self._voxwid, dtype=self._dtype, pos_c=self.pos_c, order=self._order)

@@ -125,6 +125,14 @@ APRICT_API const char *aprict_b200_last_error(void);
 /* Library version as "MAJOR.MINOR.PATCH". */
 APRICT_API const char *aprict_b200_version(void);
 
+/* Launch-shape knobs, process-wide (0 = built-in default). Keys:
+ *   0 forward-projector tile height in pixels: 8, 16 or 32;
+ *   1 backprojector voxels per thread along the slowest axis: 2 or 4;
+ *   2 backprojector brick-order wave size in CTAs per SM: 1..16.
+ * Set by the autotuner (aprict_b200/autotune.py); results never depend on them. */
+APRICT_API int aprict_b200_set_tuning(int key, int value);
+APRICT_API int aprict_b200_get_tuning(int key);
+
 /* sizeof() of a struct declared here, by its type name (0 if unknown); lets
  * bindings verify their struct mirrors without a GPU. */
 APRICT_API size_t aprict_b200_struct_size(const char *name);

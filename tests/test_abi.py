@@ -127,3 +127,22 @@ def test_volops_validation() -> None:
     assert lib.aprict_b200_vol_fill(_fake(), -1, ctypes.c_float(1.0), None) == 1
     vd = _lib.vol_desc((4, 4, 4), "C", 1.0, np.zeros(3))
     assert lib.aprict_b200_vol_softmask_cylinder(_fake(), _lib.ptr(vd), ctypes.c_float(1.5), None) == 1
+
+
+def test_tuning_knobs_validate_and_round_trip() -> None:
+    lib = _lib.lib()
+    saved = [lib.aprict_b200_get_tuning(k) for k in range(3)]
+    try:
+        for key, good, bad in [(0, (0, 8, 16, 32), (7, 64, -1)), (1, (0, 2, 4), (1, 3, 8)), (2, (0, 1, 16), (-1, 17))]:
+            for v in good:
+                assert lib.aprict_b200_set_tuning(key, v) == 0
+                assert lib.aprict_b200_get_tuning(key) == v
+            for v in bad:
+                with pytest.raises(ValueError):
+                    _lib.check(lib.aprict_b200_set_tuning(key, v), "set_tuning")
+        with pytest.raises(ValueError):
+            _lib.check(lib.aprict_b200_set_tuning(3, 0), "set_tuning")
+        assert lib.aprict_b200_get_tuning(99) == 0
+    finally:
+        for k, v in enumerate(saved):
+            lib.aprict_b200_set_tuning(k, v)

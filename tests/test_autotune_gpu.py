@@ -1,0 +1,81 @@
+"""Launch-shape knobs change speed only: every knob value gives the same result.
+
+The forward projector computes each ray independently of the tile it sits in,
+so its output is bit-identical across tile heights. The backprojector sums each
+voxel's views in the same order whatever the voxels-per-thread and wave size,
+so it is bit-identical too. The autotuner must pick allowed values and leave
+its inputs untouched.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from aprict_b200 import Volume, autotune, phantoms
+from aprict_b200.cb import flatpanel as fp
+from helpers import circular
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (40, 36, 44)
+
+
+@pytest.fixture()
+def restore_knobs():
+    saved = autotune.current()
+    yield
+    autotune.apply(saved)
+
+
+def _problem():
+    vol = Volume(phantoms.ellipsoid_volume(5, 6, SHAPE, 1.0, semi_axes_vox=(3, 12)), voxwid=1.0)
+    pg = circular(16, 120, 120, 0.537, 52, 56)
+    return vol, pg
+
+
+def test_projector_tile_height_is_bit_identical(restore_knobs) -> None:
+    vol, pg = _problem()
+    outs = []
+    for tv in autotune.FP_TILE_V:
+        autotune.apply({"fp_tile_v": tv})
+        ps = fp.ProjectionSet(pg, data=None)
+        fp.project(fp.ConfigProject(ssu=2), vol, ps, block=True)
+        outs.append(ps.data.cpu().numpy())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(fast_approx=True, approx_mode_bilinear_interpolate=True), dict(fast_approx=True)])
+def test_backprojector_shapes_are_bit_identical(restore_knobs, kw) -> None:
+    vol, pg = _problem()
+    rng = np.random.default_rng(2)
+    ps = fp.ProjectionSet(pg, data=rng.random((16, 52, 56), dtype=np.float32))
+    cfg = fp.ConfigBackproject(**kw)
+    outs = []
+    for xb in autotune.BP_XB:
+        for wave in (1, 3, 7):
+            autotune.apply({"bp_xb": xb, "bp_wave": wave})
+            v = Volume.zeros(SHAPE, voxwid=1.0)
+            fp.backproject(cfg, v, ps, block=True)
+            outs.append(v.data.cpu().numpy())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+
+
+def test_tune_picks_allowed_values_and_caches(restore_knobs, tmp_path) -> None:
+    vol, pg = _problem()
+    ps = fp.ProjectionSet(pg, data=None)
+    fp.project(fp.ConfigProject(), vol, ps, block=True)
+    before_p = ps.data.clone()
+    before_v = vol.data.clone()
+    cache = tmp_path / "tune.json"
+    choice = autotune.tune(ps, vol, cfg_bp=fp.ConfigBackproject(), cache_file=cache)
+    assert choice["fp_tile_v"] in autotune.FP_TILE_V
+    assert choice["bp_xb"] in autotune.BP_XB and choice["bp_wave"] in autotune.BP_WAVE
+    assert autotune.current()["fp_tile_v"] == choice["fp_tile_v"]
+    assert torch.equal(ps.data, before_p) and torch.equal(vol.data, before_v)
+    assert cache.exists()
+    autotune.apply({})
+    assert autotune.tune(ps, vol, cfg_bp=fp.ConfigBackproject(), cache_file=cache) == choice
