@@ -36,7 +36,11 @@ def _set(key: int, value: int) -> None:
 def current() -> dict:
     """The knobs in effect (0 = built-in default)."""
     lib = _lib.lib()
-    return {"fp_tile_v": lib.aprict_b200_get_tuning(0), "bp_xb": lib.aprict_b200_get_tuning(1), "bp_wave": lib.aprict_b200_get_tuning(2)}
+    return {
+        "fp_tile_v": lib.aprict_b200_get_tuning(KEY_FP_TILE_V),
+        "bp_xb": lib.aprict_b200_get_tuning(KEY_BP_XB),
+        "bp_wave": lib.aprict_b200_get_tuning(KEY_BP_WAVE),
+    }
 
 
 def apply(choice: dict) -> None:

@@ -33,6 +33,8 @@ struct BPParams {
     uint32_t n_views, nu, nv;
     int64_t stride_view;
     int su, sv;  // u, v element strides (in-view offsets are checked to fit 32 bits)
+    float fnu1, fnv1;  // nu + 1, nv + 1: clamp bounds for the rounded pixel index
+    float tie;         // |f - round(f)| above this is settled in FP64
     const float *projs;
     float *vol;
     const float *mult;
@@ -57,12 +59,27 @@ struct BPParams {
     uint32_t *status;
 };
 
-// Pixel value with the reference's zero-order rule (get_zero_interp,
-// CB_backproject.cu:256-271): index floor(f + 0.5). When f + 0.5 lies within
-// kRefine of an integer the FP32 estimate (error ~1e-4 pixel) cannot be
-// trusted to pick the pixel an exact evaluation picks, so the choice is made
-// again in FP64 from the voxel's FP64 position.
-constexpr float kRefine = 2e-3f;
+// Pixel index with the reference's zero-order rule (get_zero_interp,
+// CB_backproject.cu:256-271): floor(f + 0.5). The FP32 estimate of f has an
+// error of ~1.1e-4 pixel on a 384-pixel detector plus ~1 ulp of f from the
+// approximate reciprocal (emulated over a 360-view circular scan), growing
+// with the detector size. When f lies within refine = 2e-3 * max(1, n/1024)
+// of a half-integer the choice is made again in FP64 from the voxel's exact
+// position; the kernel receives tie = 1/2 - refine.
+
+// x + 1.5 * 2^23 rounds x to the nearest integer (ties to even), which then
+// sits in the low mantissa bits; valid for |x| < 2^22 (the clamp ensures it,
+// and sends NaN to lo). frac = x - index, in [-1/2, 1/2]. Round-to-even and
+// floor(x + 1/2) differ only at exact half-integers, which the caller always
+// refines.
+constexpr float kMagic = 12582912.0f;
+
+__device__ __forceinline__ int round_index(float x, float lo, float hi, float &frac) {
+    const float xc = fminf(fmaxf(x, lo), hi);
+    const float t = __fadd_rn(xc, kMagic);
+    frac = __fsub_rn(xc, __fsub_rn(t, kMagic));
+    return __float_as_int(t) - 0x4B400000;
+}
 
 // FP64 position of a voxel (centre + sub-sample offset) relative to the
 // volume centre, from its integer indices: exact in double.
@@ -70,27 +87,17 @@ struct VoxRef {
     double x, y, z;
 };
 
-__device__ __forceinline__ float refine_nearest(const BPParams &P, const float *pvw, const ab_bpview_d &c,
-                                                const VoxRef &r) {
-    const double D = fma(c.den[0], r.x, fma(c.den[1], r.y, fma(c.den[2], r.z, c.den[3])));
-    const double du = fma(c.nu[0], r.x, fma(c.nu[1], r.y, fma(c.nu[2], r.z, c.nu[3]))) / D;
-    const double dv = fma(c.nv[0], r.x, fma(c.nv[1], r.y, fma(c.nv[2], r.z, c.nv[3]))) / D;
-    const double gu = floor(du + 0.5), gv = floor(dv + 0.5);
-    if (!(gu >= 0.0 && gu < (double)P.nu && gv >= 0.0 && gv < (double)P.nv)) return 0.f;
-    return __ldg(pvw + ((int)gu * P.su + (int)gv * P.sv));
-}
-
-__device__ __forceinline__ float fetch_nearest(const BPParams &P, const float *pvw, const ab_bpview_d &c,
-                                               float fu, float fv, const VoxRef &r) {
-    const float gu = fu + 0.5f, gv = fv + 0.5f;
-    const float lu = floorf(gu), lv = floorf(gv);
-    // |frac - 1/2| <= 1/2 - kRefine on both axes, written so that NaN fails
-    if (!(fabsf(gu - lu - 0.5f) <= 0.5f - kRefine && fabsf(gv - lv - 0.5f) <= 0.5f - kRefine))
-        return refine_nearest(P, pvw, c, r);
-    // float -> int saturates, so out-of-range values fail the unsigned test
-    const int iu = (int)lu, iv = (int)lv;
-    if ((unsigned)iu >= P.nu || (unsigned)iv >= P.nv) return 0.f;
-    return __ldg(pvw + (iu * P.su + iv * P.sv));
+// floor(N/D + 1/2) in FP64 given the FP32 estimate i of the rounded value
+// and its fraction (f - i): the answer is i or its neighbour on the side of
+// frac, decided by the sign of N - (i +- 1/2) D without a division.
+__device__ __forceinline__ int refine_index(const double *num, const double *den, const VoxRef &r, int i, float frac) {
+    const double N = fma(num[0], r.x, fma(num[1], r.y, fma(num[2], r.z, num[3])));
+    const double D = fma(den[0], r.x, fma(den[1], r.y, fma(den[2], r.z, den[3])));
+    if (!(D != 0.0) || !(fabs(N) < 1e300)) return -1;
+    const double h = frac > 0.f ? (double)i + 0.5 : (double)i - 0.5;
+    const double e = fma(-h, D, N);  // (N/D - h) * D
+    if (frac > 0.f) return (D > 0.0 ? e >= 0.0 : e <= 0.0) ? i + 1 : i;
+    return (D > 0.0 ? e < 0.0 : e > 0.0) ? i - 1 : i;
 }
 
 // Bilinear rule of get_bilinear_interp (CB_backproject.cu:221-254), same
@@ -198,9 +205,6 @@ __global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(BPPar
 #pragma unroll
     for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
 
-    // Volume centre in FP64 (exact: corner and voxwid are floats, n an integer).
-    const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
-                    P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
     const bool needZ = P.pL != 0 || P.pV != 0;
     const int n_sub = P.ssx * P.ssy * P.ssz;
@@ -216,6 +220,9 @@ __global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(BPPar
                     const int cn = (int)min((uint32_t)kChunk, P.n_views - v0);
                     __syncthreads();
                     for (int t = threadIdx.x; t < cn; t += kThreads) {
+                        // Volume centre in FP64 (exact: corner and voxwid are floats, n an integer).
+                        const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
+                                        P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
                         const aprict_proj_spec sp = P.specs[v0 + t];
                         if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t], kNear ? &svd[t] : nullptr) && P.status)
                             atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
@@ -237,111 +244,170 @@ __global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(BPPar
                             Zb = dot4(b.zl, X0, Y0, Z0);
                             dZ = (a2 == 0 ? b.zl.x : (a2 == 1 ? b.zl.y : b.zl.z)) * vw;
                         }
+                        if constexpr (EXACT) {
 #pragma unroll
-                        for (int k = 0; k < kXB; ++k) {
-                            if (!live[k]) continue;
-                            const float kf = (float)k;
-                            const float D = fmaf(kf, dD, D0);
-                            const float rD = rcp_fast(D);
-                            const float fu = fmaf(kf, dNu, Nu0) * rD;
-                            const float fv = fmaf(kf, dNv, Nv0) * rD;
-                            float s;
-                            if (EXACT) {
-                                // Footprint: bounding box of the 8 projected corners.
-                                const ab_bpview_exact e = sx[t];
-                                const float h = 0.5f * vw;
-                                const float hu[3] = {b.nu.x * h, b.nu.y * h, b.nu.z * h};
-                                const float hv[3] = {b.nv.x * h, b.nv.y * h, b.nv.z * h};
-                                const float hd[3] = {b.den.x * h, b.den.y * h, b.den.z * h};
-                                const float Nu = fmaf(kf, dNu, Nu0), Nv = fmaf(kf, dNv, Nv0);
-                                float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+                            for (int k = 0; k < kXB; ++k) {
+                                if (!live[k]) continue;
+                                const float kf = (float)k;
+                                const float D = fmaf(kf, dD, D0);
+                                const float rD = rcp_fast(D);
+                                const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                const float fv = fmaf(kf, dNv, Nv0) * rD;
+                                float s;
+                                {
+                                    // Footprint: bounding box of the 8 projected corners.
+                                    const ab_bpview_exact e = sx[t];
+                                    const float h = 0.5f * vw;
+                                    const float hu[3] = {b.nu.x * h, b.nu.y * h, b.nu.z * h};
+                                    const float hv[3] = {b.nv.x * h, b.nv.y * h, b.nv.z * h};
+                                    const float hd[3] = {b.den.x * h, b.den.y * h, b.den.z * h};
+                                    const float Nu = fmaf(kf, dNu, Nu0), Nv = fmaf(kf, dNv, Nv0);
+                                    float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
 #pragma unroll
-                                for (int c = 0; c < 8; ++c) {
-                                    const float sx_ = (c & 4) ? 1.f : -1.f, sy_ = (c & 2) ? 1.f : -1.f,
-                                                sz_ = (c & 1) ? 1.f : -1.f;
-                                    const float dd = D + sx_ * hd[0] + sy_ * hd[1] + sz_ * hd[2];
-                                    const float rr = rcp_fast(dd);
-                                    const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * rr;
-                                    const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * rr;
-                                    umin = fminf(umin, uu);
-                                    umax = fmaxf(umax, uu);
-                                    vmin = fminf(vmin, vv);
-                                    vmax = fmaxf(vmax, vv);
-                                }
-                                const int ulo = max(0, (int)ceilf(umin - 1e-3f));
-                                const int uhi = min((int)P.nu - 1, (int)floorf(umax + 1e-3f));
-                                const int vlo = max(0, (int)ceilf(vmin - 1e-3f));
-                                const int vhi = min((int)P.nv - 1, (int)floorf(vmax + 1e-3f));
-                                // Ray origin relative to this voxel's centre.
-                                float cx[3] = {X0, Y0, Z0};
-                                cx[a2] += kf * vw;
-                                const float r0x = e.s.x - cx[0], r0y = e.s.y - cx[1], r0z = e.s.z - cx[2];
-                                s = 0.f;
-                                for (int iu = ulo; iu <= uhi; ++iu) {
-                                    const float dux = fmaf(e.u.x, (float)iu, e.d0.x);
-                                    const float duy = fmaf(e.u.y, (float)iu, e.d0.y);
-                                    const float duz = fmaf(e.u.z, (float)iu, e.d0.z);
-                                    for (int iv = vlo; iv <= vhi; ++iv) {
-                                        const float dx = fmaf(e.v.x, (float)iv, dux);
-                                        const float dy = fmaf(e.v.y, (float)iv, duy);
-                                        const float dz = fmaf(e.v.z, (float)iv, duz);
-                                        float a_lo = 0.f, a_hi = 3.0e38f;
-                                        bool miss = false;
-                                        if (dx != 0.f) {
-                                            const float inv = rcp_fast(dx);
-                                            const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
-                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                        } else {
-                                            miss |= fabsf(r0x) > h;
-                                        }
-                                        if (dy != 0.f) {
-                                            const float inv = rcp_fast(dy);
-                                            const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
-                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                        } else {
-                                            miss |= fabsf(r0y) > h;
-                                        }
-                                        if (dz != 0.f) {
-                                            const float inv = rcp_fast(dz);
-                                            const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
-                                            a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                            a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                        } else {
-                                            miss |= fabsf(r0z) > h;
-                                        }
-                                        if (miss || !(a_hi > a_lo)) continue;
-                                        const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
-                                        const float pv = P.all_ones ? 1.f : __ldg(pvw + (iu * P.su + iv * P.sv));
-                                        s = fmaf(pv, chord, s);
+                                    for (int c = 0; c < 8; ++c) {
+                                        const float sx_ = (c & 4) ? 1.f : -1.f, sy_ = (c & 2) ? 1.f : -1.f,
+                                                    sz_ = (c & 1) ? 1.f : -1.f;
+                                        const float dd = D + sx_ * hd[0] + sy_ * hd[1] + sz_ * hd[2];
+                                        const float rr = rcp_fast(dd);
+                                        const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * rr;
+                                        const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * rr;
+                                        umin = fminf(umin, uu);
+                                        umax = fmaxf(umax, uu);
+                                        vmin = fminf(vmin, vv);
+                                        vmax = fmaxf(vmax, vv);
                                     }
+                                    const int ulo = max(0, (int)ceilf(umin - 1e-3f));
+                                    const int uhi = min((int)P.nu - 1, (int)floorf(umax + 1e-3f));
+                                    const int vlo = max(0, (int)ceilf(vmin - 1e-3f));
+                                    const int vhi = min((int)P.nv - 1, (int)floorf(vmax + 1e-3f));
+                                    // Ray origin relative to this voxel's centre.
+                                    float cx[3] = {X0, Y0, Z0};
+                                    cx[a2] += kf * vw;
+                                    const float r0x = e.s.x - cx[0], r0y = e.s.y - cx[1], r0z = e.s.z - cx[2];
+                                    s = 0.f;
+                                    for (int iu = ulo; iu <= uhi; ++iu) {
+                                        const float dux = fmaf(e.u.x, (float)iu, e.d0.x);
+                                        const float duy = fmaf(e.u.y, (float)iu, e.d0.y);
+                                        const float duz = fmaf(e.u.z, (float)iu, e.d0.z);
+                                        for (int iv = vlo; iv <= vhi; ++iv) {
+                                            const float dx = fmaf(e.v.x, (float)iv, dux);
+                                            const float dy = fmaf(e.v.y, (float)iv, duy);
+                                            const float dz = fmaf(e.v.z, (float)iv, duz);
+                                            float a_lo = 0.f, a_hi = 3.0e38f;
+                                            bool miss = false;
+                                            if (dx != 0.f) {
+                                                const float inv = rcp_fast(dx);
+                                                const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
+                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                            } else {
+                                                miss |= fabsf(r0x) > h;
+                                            }
+                                            if (dy != 0.f) {
+                                                const float inv = rcp_fast(dy);
+                                                const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
+                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                            } else {
+                                                miss |= fabsf(r0y) > h;
+                                            }
+                                            if (dz != 0.f) {
+                                                const float inv = rcp_fast(dz);
+                                                const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
+                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                            } else {
+                                                miss |= fabsf(r0z) > h;
+                                            }
+                                            if (miss || !(a_hi > a_lo)) continue;
+                                            const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
+                                            const float pv = P.all_ones ? 1.f : __ldg(pvw + (iu * P.su + iv * P.sv));
+                                            s = fmaf(pv, chord, s);
+                                        }
+                                    }
+                                    if (needZ) s *= zpow(P, b, fmaf(kf, dZ, Zb));
                                 }
-                                if (needZ) s *= zpow(P, b, fmaf(kf, dZ, Zb));
-                            } else {
-                                // fast mode: weight (|p - s| / |x - s|)^2 voxwid^3 / pixel area
-                                // (:648-690), or the direct-raycast weights (:512-646)
+                                if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
+                                acc[k] += s;
+                            }
+                        } else {
+                            // Fast modes: one branch-free pass over the thread's voxels;
+                            // voxel-views that need more (a near-tie pixel choice, the
+                            // detector-edge taper band) are flagged and finished in a rare
+                            // second pass, so the common path has no divergent branches.
+                            unsigned pending = 0;
+#pragma unroll
+                            for (int k = 0; k < kXB; ++k) {
+                                const float kf = (float)k;
+                                const float D = fmaf(kf, dD, D0);
+                                const float rD = rcp_fast(D);
+                                const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                const float fv = fmaf(kf, dNv, Nv0) * rD;
                                 float w = RAYCAST ? 1.f : b.kfast * rD * rD;
                                 if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
+                                // inner: inside the taper's flat box, which lies inside the
+                                // detector (|f - c| <= n/2 without a taper)
+                                const bool inner = fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv;
                                 float pv = 0.f;
-                                if (w != 0.f) {
+                                bool fast;
+                                if (BILIN) {
+                                    fast = inner;
+                                    pv = fetch_bilinear(P, pvw, fu, fv);
+                                    pv = live[k] && fast ? pv : 0.f;
+                                } else {
+                                    // Inside the detector box |f| < 2^22, so the rounding trick
+                                    // needs no clamp; a pixel at most 1/2 - refine from f is
+                                    // then a valid index (the box edges are half-integers).
+                                    const float tu = __fadd_rn(fu, kMagic), tv = __fadd_rn(fv, kMagic);
+                                    const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
+                                    const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
+                                    fast = inner && fabsf(du) <= P.tie && fabsf(dv) <= P.tie;
+                                    // pixel offset from the rounded indices (bits - magic)
+                                    const int off = (__float_as_int(tu) - 0x4B400000) * P.su + (__float_as_int(tv) - 0x4B400000) * P.sv;
+                                    if (live[k] && fast) pv = __ldg(pvw + off);
+                                }
+                                acc[k] = fmaf(pv, w, acc[k]);
+                                pending |= (live[k] && !fast) ? 1u << k : 0u;
+                            }
+                            if (pending != 0u) {
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    if (!((pending >> k) & 1u)) continue;
+                                    const float kf = (float)k;
+                                    const float D = fmaf(kf, dD, D0);
+                                    const float rD = rcp_fast(D);
+                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                    const float fv = fmaf(kf, dNv, Nv0) * rD;
+                                    float w = RAYCAST ? 1.f : b.kfast * rD * rD;
+                                    if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
+                                    float pv;
                                     if (BILIN) {
                                         pv = fetch_bilinear(P, pvw, fu, fv);
                                     } else {
-                                        int id[3];
-                                        id[a0] = i0;
-                                        id[a1] = i1;
-                                        id[a2] = i2b + k;
-                                        const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
-                                                        ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
-                                                        ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
-                                        pv = fetch_nearest(P, pvw, svd[kNear ? t : 0], fu, fv, vr);
+                                        float du, dv;
+                                        int iu = round_index(fu, -2.f, P.fnu1, du);
+                                        int iv = round_index(fv, -2.f, P.fnv1, dv);
+                                        const bool tu = fabsf(du) > P.tie, tv = fabsf(dv) > P.tie;
+                                        if (tu || tv) {
+                                            int id[3];
+                                            id[a0] = i0;
+                                            id[a1] = i1;
+                                            id[a2] = i2b + k;
+                                            const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                            ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                            ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
+                                            const ab_bpview_d &c = svd[kNear ? t : 0];
+                                            if (tu) iu = refine_index(c.nu, c.den, vr, iu, du);
+                                            if (tv) iv = refine_index(c.nv, c.den, vr, iv, dv);
+                                        }
+                                        const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
+                                        pv = inb ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
                                     }
+                                    float s = pv * w;
+                                    if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
+                                    acc[k] += s;
                                 }
-                                s = pv * w;
                             }
-                            if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
-                            acc[k] += s;
                         }
                     }
                 }
@@ -405,6 +471,8 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     if (specs_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null view specs");
     if (multiplier_dev && (reinterpret_cast<uintptr_t>(multiplier_dev) & 3u))
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "multiplier pointer not 4-byte aligned");
+    if (pd->nu > (1u << 21) || pd->nv > (1u << 21))
+        return ab_fail(APRICT_ERR_TOO_LARGE, "backprojection supports at most 2^21 detector pixels per axis");
     if ((int64_t)(pd->nu - 1) * pd->stride_u + (int64_t)(pd->nv - 1) * pd->stride_v + 1 > 0x7fffffffLL)
         return ab_fail(APRICT_ERR_TOO_LARGE, "one projection image spans more than 2^31 elements");
 
@@ -416,6 +484,9 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.stride_view = pd->stride_view;
     P.su = (int)pd->stride_u;
     P.sv = (int)pd->stride_v;
+    P.fnu1 = (float)pd->nu + 1.f;
+    P.fnv1 = (float)pd->nv + 1.f;
+    P.tie = 0.5f - 2e-3f * fmaxf(1.f, (float)(pd->nu > pd->nv ? pd->nu : pd->nv) / 1024.f);
     P.projs = projs_dev;
     P.vol = vol_dev;
     P.mult = multiplier_dev;
@@ -452,7 +523,7 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     P.ssz = (int)cfg->ssz;
     P.status = status_dev;
 
-    const int xb = ab_tuning_get(AB_TUNE_BP_XB) == 2 ? 2 : 4;
+    const int xb = ab_tuning_get(AB_TUNE_BP_XB) == 4 ? 4 : 2;
     const int kXB = xb;
     const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
     P.gb[0] = (n0 + 31) / 32;

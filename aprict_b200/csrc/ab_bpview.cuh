@@ -31,7 +31,8 @@ struct ab_bpview {
     float halfv; // nv / 2
     float inv_halfu, inv_halfv;
     // Edge taper: |fu - cu0| <= tap_ru and |fv - cv0| <= tap_rv guarantees a
-    // factor of exactly 1 (a margin of 1e-5 keeps it conservative).
+    // factor of exactly 1 (a margin of 1e-5 keeps it conservative). Without a
+    // taper the box is the detector itself (half-widths nu/2, nv/2).
     float cu0, cv0, tap_ru, tap_rv;
 };
 
@@ -89,7 +90,7 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     o.inv_halfv = (float)(2.0 / (double)sp.nv);
     o.cu0 = (float)hu;
     o.cv0 = (float)hv;
-    const double keep = sep > 0.f ? (1.0 - (double)sep) * (1.0 - 1e-5) : 1e30;
+    const double keep = sep > 0.f ? (1.0 - (double)sep) * (1.0 - 1e-5) : 1.0;
     o.tap_ru = (float)(0.5 * (double)sp.nu * keep);
     o.tap_rv = (float)(0.5 * (double)sp.nv * keep);
     return true;

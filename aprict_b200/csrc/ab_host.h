@@ -22,7 +22,7 @@ int ab_check_projs(const aprict_proj_desc *p, const void *ptr, const char *name)
 // Launch-shape knobs (set by the autotuner through aprict_b200_set_tuning).
 enum {
     AB_TUNE_FP_TILE_V = 0,  // forward projector tile height in pixels (0 = auto, 8, 16, 32)
-    AB_TUNE_BP_XB = 1,      // backprojector voxels per thread (0 = auto = 4, 2, 4)
+    AB_TUNE_BP_XB = 1,      // backprojector voxels per thread (0 = auto = 2, 2, 4)
     AB_TUNE_BP_WAVE = 2,    // backprojector super-brick size in CTAs per SM (0 = auto = 3)
     AB_TUNE_COUNT = 3
 };
