@@ -1,7 +1,7 @@
 """Launch-shape autotuner.
 
 Times a few candidate launch shapes of the forward projector (detector tile
-height) and the backprojector (voxels per thread, size of the brick-ordered
+height, warp patch shape) and the backprojector (voxels per thread, size of the brick-ordered
 wave) on the caller's own problem with CUDA events, keeps the fastest, and
 applies it through ``aprict_b200_set_tuning``. Results never depend on these
 knobs; only speed does. Choices are cached per problem signature (in memory,
@@ -20,8 +20,9 @@ from . import _lib
 from .cb import flatpanel as fp
 from .volume import Volume
 
-KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE = 0, 1, 2
+KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V = 0, 1, 2, 3
 FP_TILE_V = (8, 16, 32)
+FP_WARP_V = (8, 16, 32)
 BP_XB = (2, 4)
 BP_WAVE = (2, 3, 4, 6)
 
@@ -38,6 +39,7 @@ def current() -> dict:
     lib = _lib.lib()
     return {
         "fp_tile_v": lib.aprict_b200_get_tuning(KEY_FP_TILE_V),
+        "fp_warp_v": lib.aprict_b200_get_tuning(KEY_FP_WARP_V),
         "bp_xb": lib.aprict_b200_get_tuning(KEY_BP_XB),
         "bp_wave": lib.aprict_b200_get_tuning(KEY_BP_WAVE),
     }
@@ -46,6 +48,7 @@ def current() -> dict:
 def apply(choice: dict) -> None:
     """Apply a choice returned by :func:`tune`."""
     _set(KEY_FP_TILE_V, choice.get("fp_tile_v", 0))
+    _set(KEY_FP_WARP_V, choice.get("fp_warp_v", 0))
     _set(KEY_BP_XB, choice.get("bp_xb", 0))
     _set(KEY_BP_WAVE, choice.get("bp_wave", 0))
 
@@ -99,10 +102,15 @@ def tune(
     cfg_fp = fp.ConfigProject()
     times = {}
     for tv in FP_TILE_V:
-        _set(KEY_FP_TILE_V, tv)
-        times[tv] = _time(lambda: fp.project(cfg_fp, volume, scratch_p), reps)
-    choice["fp_tile_v"] = min(times, key=times.get)
-    choice["fp_ms"] = round(times[choice["fp_tile_v"]], 4)
+        for wv in FP_WARP_V:
+            if wv > tv:
+                continue
+            _set(KEY_FP_TILE_V, tv)
+            _set(KEY_FP_WARP_V, wv)
+            times[(tv, wv)] = _time(lambda: fp.project(cfg_fp, volume, scratch_p), reps)
+    best_fp = min(times, key=times.get)
+    choice["fp_tile_v"], choice["fp_warp_v"] = best_fp
+    choice["fp_ms"] = round(times[best_fp], 4)
     if cfg_bp is not None:
         scratch_v = volume.zeroed_copy()
         best = None

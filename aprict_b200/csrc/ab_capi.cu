@@ -13,7 +13,7 @@ static_assert(sizeof(aprict_project_config) == 16, "project_config layout");
 static_assert(sizeof(aprict_backproject_config) == 76, "backproject_config layout");
 
 static thread_local char g_last_error[512] = "";
-static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0};
+static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0, 0};
 
 int ab_tuning_get(int key) { return key >= 0 && key < AB_TUNE_COUNT ? __atomic_load_n(&g_tuning[key], __ATOMIC_RELAXED) : 0; }
 
@@ -99,6 +99,7 @@ int aprict_b200_set_tuning(int key, int value) {
     switch (key) {
         case AB_TUNE_FP_TILE_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
         case AB_TUNE_BP_XB: ok = value == 0 || value == 2 || value == 4; break;
+        case AB_TUNE_FP_WARP_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
         default: ok = value >= 0 && value <= 16; break;
     }
     if (!ok) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "tuning value %d not allowed for key %d", value, key);

@@ -24,7 +24,8 @@ enum {
     AB_TUNE_FP_TILE_V = 0,  // forward projector tile height in pixels (0 = auto, 8, 16, 32)
     AB_TUNE_BP_XB = 1,      // backprojector voxels per thread (0 = auto = 2, 2, 4)
     AB_TUNE_BP_WAVE = 2,    // backprojector super-brick size in CTAs per SM (0 = auto = 3)
-    AB_TUNE_COUNT = 3
+    AB_TUNE_FP_WARP_V = 3,  // forward projector lanes of a warp along v (0 = auto = 8, 8, 16, 32)
+    AB_TUNE_COUNT = 4
 };
 int ab_tuning_get(int key);
 

@@ -6,7 +6,7 @@
 // scaled by multiply_before_adding (:394) and accumulated (:411).
 //
 // B200 layout: a CTA covers a 2-D detector tile of one view and each warp a
-// 4 (u) x 8 (v) pixel patch, so the rays of a warp are spatially coherent and
+// 4 (u) x 8 (v) pixel patch (2 x 16 or 1 x 32 as tuned), so the rays of a warp are spatially coherent and
 // their voxel gathers hit the same L1 lines; 8 consecutive v per row make the
 // output access one 32-byte sector.
 #include <cuda_runtime.h>
@@ -20,6 +20,7 @@ constexpr int kThreads = 256;
 
 struct TileMap {
     int tile_u, tile_v;  // tile extents in pixels
+    int warp_v;          // lanes of a warp along v (warp patch: 32/warp_v along u)
     int ntu, ntv;        // number of tiles along u, v
 };
 
@@ -30,6 +31,10 @@ TileMap make_tiles(uint32_t nu, uint32_t nv) {
     t.tile_v = nv >= 16 ? 16 : (nv >= 8 ? 8 : 1);
     const int want = ab_tuning_get(AB_TUNE_FP_TILE_V);  // autotuner override: 8, 16 or 32
     if ((want == 8 || want == 16 || want == 32) && nv >= 8) t.tile_v = want;
+    // Warp patch: 4 (u) x 8 (v) by default; the autotuner may try 2 x 16 or 1 x 32.
+    const int wv = ab_tuning_get(AB_TUNE_FP_WARP_V);
+    t.warp_v = (wv == 16 || wv == 32) ? wv : 8;
+    if (t.tile_v > 1 && t.warp_v > t.tile_v) t.tile_v = t.warp_v;
     t.tile_u = kThreads / t.tile_v;
     t.ntu = (int)((nu + t.tile_u - 1) / t.tile_u);
     t.ntv = (int)((nv + t.tile_v - 1) / t.tile_v);
@@ -52,10 +57,10 @@ __device__ __forceinline__ void block_tile(const TileMap &tm, uint32_t n_views, 
         iv = tv;
     } else {
         const int lane = t & 31, warp = t >> 5;
-        const int wv_per = tm.tile_v / 8;  // warps along v in the tile
+        const int wv_per = tm.tile_v / tm.warp_v;  // warps along v in the tile
         const int wu = warp / wv_per, wv = warp % wv_per;
-        iu = tu * tm.tile_u + wu * 4 + (lane >> 3);
-        iv = tv * tm.tile_v + wv * 8 + (lane & 7);
+        iu = tu * tm.tile_u + wu * (32 / tm.warp_v) + lane / tm.warp_v;
+        iv = tv * tm.tile_v + wv * tm.warp_v + lane % tm.warp_v;
     }
 }
 

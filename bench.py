@@ -291,7 +291,8 @@ def run_ours(args) -> dict:
     fp_gbs = fp_bytes / (t_fp * 1e-3) / 1e9
     bp_gbs = bp_bytes / (t_bp * 1e-3) / 1e9
     dom = "project_siddon" if t_fp >= t_bp else "backproject"
-    traffic = load_traffic().get(f"{dom}:{args.workload}")
+    tr = load_traffic().get(f"{dom}:{args.workload}")
+    traffic = tr["dram_bytes"] if tr else None
     roof = {
         "bound": "hbm",
         "kernel": dom,
@@ -301,6 +302,8 @@ def run_ours(args) -> dict:
         "frac": round((fp_gbs if dom == "project_siddon" else bp_gbs) / peak, 4),
         "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s",
         "traffic": traffic,
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/)",
+        "algorithmic_bytes": round(fp_bytes if dom == "project_siddon" else bp_bytes),
         "model": "FP: 4 B per ray/voxel segment + 8 B per ray; BP: 4 B per voxel-view + 12 B per voxel",
     }
     out = {

@@ -1,7 +1,7 @@
 """Launch-shape knobs change speed only: every knob value gives the same result.
 
 The forward projector computes each ray independently of the tile it sits in,
-so its output is bit-identical across tile heights. The backprojector's wave
+so its output is bit-identical across tile heights and warp patch shapes. The backprojector's wave
 size only reorders CTAs, so it is bit-identical too; its voxels-per-thread
 count changes where the per-view affine terms are stepped from (a thread's
 first voxel), so results across that knob agree to float rounding (rel L2
@@ -36,14 +36,15 @@ def _problem():
     return vol, pg
 
 
-def test_projector_tile_height_is_bit_identical(restore_knobs) -> None:
+def test_projector_tile_shapes_are_bit_identical(restore_knobs) -> None:
     vol, pg = _problem()
     outs = []
     for tv in autotune.FP_TILE_V:
-        autotune.apply({"fp_tile_v": tv})
-        ps = fp.ProjectionSet(pg, data=None)
-        fp.project(fp.ConfigProject(ssu=2), vol, ps, block=True)
-        outs.append(ps.data.cpu().numpy())
+        for wv in autotune.FP_WARP_V:
+            autotune.apply({"fp_tile_v": tv, "fp_warp_v": wv})
+            ps = fp.ProjectionSet(pg, data=None)
+            fp.project(fp.ConfigProject(ssu=2), vol, ps, block=True)
+            outs.append(ps.data.cpu().numpy())
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
 
@@ -77,7 +78,7 @@ def test_tune_picks_allowed_values_and_caches(restore_knobs, tmp_path) -> None:
     before_v = vol.data.clone()
     cache = tmp_path / "tune.json"
     choice = autotune.tune(ps, vol, cfg_bp=fp.ConfigBackproject(), cache_file=cache)
-    assert choice["fp_tile_v"] in autotune.FP_TILE_V
+    assert choice["fp_tile_v"] in autotune.FP_TILE_V and choice["fp_warp_v"] in autotune.FP_WARP_V
     assert choice["bp_xb"] in autotune.BP_XB and choice["bp_wave"] in autotune.BP_WAVE
     assert autotune.current()["fp_tile_v"] == choice["fp_tile_v"]
     assert torch.equal(ps.data, before_p) and torch.equal(vol.data, before_v)
