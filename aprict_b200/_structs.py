@@ -99,6 +99,16 @@ quadric = np.dtype(
     ]
 )
 
+# One scan of a batch (aprict_scan): the arguments of one one-scan call.
+scan = np.dtype(
+    {
+        "names": ["specs_dev", "projs", "projs_dev", "base_dev", "vol", "vol_dev", "multiplier_dev", "status_dev"],
+        "formats": ["<u8", proj_desc, "<u8", "<u8", vol_desc, "<u8", "<u8", "<u8"],
+        "offsets": [0, 8, 48, 56, 64, 96, 104, 112],
+        "itemsize": 120,
+    }
+)
+
 # name in the C library -> numpy dtype, checked against sizeof() in tests.
 ABI_STRUCTS = {
     "aprict_proj_spec": proj_spec,
@@ -108,4 +118,5 @@ ABI_STRUCTS = {
     "aprict_backproject_config": backproject_config,
     "aprict_forbild_shape": forbild_shape,
     "aprict_quadric": quadric,
+    "aprict_scan": scan,
 }

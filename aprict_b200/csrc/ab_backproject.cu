@@ -1,433 +1,17 @@
 // ab_backproject.cu -- voxel-driven cone-beam backprojection, all views in
-// one launch.
-//
-// Replaces backproject_CB_voltex<float,float>
-// (src/aprict/data/cusrc/CB_backproject.cu:952-1027; per-voxel body
-// _backproject_CB_getval :313-733) and the host loop that launches it once per
-// 10 views with the 640-byte proj_chunk_spec_maxlen10 passed by value
-// (src/aprict/cb/flatpanel.py:1192-1278).
-//
-// B200 layout: a warp covers 32 consecutive voxels along the volume's fastest
-// axis, so the final read-modify-write of the volume is one coalesced 128-byte
-// line per warp, and for circular scans the 32 voxel centres project onto one
-// detector column -- the projection gathers of a warp fall into 2-3 lines.
-// Each thread carries XB voxels along the slowest axis (independent
-// accumulators for ILP). Per-view coefficients (ab_bpview) are derived once per
-// CTA into shared memory and read as uniform broadcasts; the volume is read and
-// written exactly once per call instead of once per 10 views. CTAs are issued
-// in brick order (all of the fastest axis x a compact block of the other two)
-// so that the CTAs resident at one time project onto a small part of each
-// view and the projection data they gather stays in L2.
+// one launch (one scan). The work unit lives in ab_bpbrick.cuh.
 #include <cuda_runtime.h>
 
-#include "ab_bpview.cuh"
-#include "ab_host.h"
+#include "ab_bpbrick.cuh"
 
 namespace {
 
-constexpr int kThreads = 256;  // 32 (fast axis) x 8 (middle axis)
-constexpr int kChunk = 128;    // views per shared-memory chunk
+using namespace ab_bp;
 
-struct BPParams {
-    const aprict_proj_spec *specs;
-    uint32_t n_views, nu, nv;
-    int64_t stride_view;
-    int su, sv;  // u, v element strides (in-view offsets are checked to fit 32 bits)
-    float fnu1, fnv1;  // nu + 1, nv + 1: clamp bounds for the rounded pixel index
-    float tie;         // |f - round(f)| above this is settled in FP64
-    const float *projs;
-    float *vol;
-    const float *mult;
-    int n[3];        // volume shape (x, y, z)
-    int64_t vs[3];   // element strides (x, y, z)
-    float voxwid;
-    float c0[3];     // volume centre (world)
-    double cornerd[3];
-    double vwd;
-    // brick-ordered CTA remap
-    int gb[3];       // blocks along fastest, middle, slowest axis
-    int sb1, sb2;    // super-brick extent in blocks along middle, slowest axis
-    int nsb1;        // super-bricks along the middle axis
-    // config
-    int mask;
-    float mask_r2;
-    int all_ones;
-    float sep, inv_sep;
-    int pL, pV;
-    float val;
-    int ssx, ssy, ssz;
-    uint32_t *status;
-};
-
-// Pixel index with the reference's zero-order rule (get_zero_interp,
-// CB_backproject.cu:256-271): floor(f + 0.5). The FP32 estimate of f has an
-// error of ~1.1e-4 pixel on a 384-pixel detector plus ~1 ulp of f from the
-// approximate reciprocal (emulated over a 360-view circular scan), growing
-// with the detector size. When f lies within refine = 2e-3 * max(1, n/1024)
-// of a half-integer the choice is made again in FP64 from the voxel's exact
-// position; the kernel receives tie = 1/2 - refine.
-
-// x + 1.5 * 2^23 rounds x to the nearest integer (ties to even), which then
-// sits in the low mantissa bits; valid for |x| < 2^22 (the clamp ensures it,
-// and sends NaN to lo). frac = x - index, in [-1/2, 1/2]. Round-to-even and
-// floor(x + 1/2) differ only at exact half-integers, which the caller always
-// refines.
-constexpr float kMagic = 12582912.0f;
-
-__device__ __forceinline__ int round_index(float x, float lo, float hi, float &frac) {
-    const float xc = fminf(fmaxf(x, lo), hi);
-    const float t = __fadd_rn(xc, kMagic);
-    frac = __fsub_rn(xc, __fsub_rn(t, kMagic));
-    return __float_as_int(t) - 0x4B400000;
-}
-
-// FP64 position of a voxel (centre + sub-sample offset) relative to the
-// volume centre, from its integer indices: exact in double.
-struct VoxRef {
-    double x, y, z;
-};
-
-// floor(N/D + 1/2) in FP64 given the FP32 estimate i of the rounded value
-// and its fraction (f - i): the answer is i or its neighbour on the side of
-// frac, decided by the sign of N - (i +- 1/2) D without a division.
-__device__ __forceinline__ int refine_index(const double *num, const double *den, const VoxRef &r, int i, float frac) {
-    const double N = fma(num[0], r.x, fma(num[1], r.y, fma(num[2], r.z, num[3])));
-    const double D = fma(den[0], r.x, fma(den[1], r.y, fma(den[2], r.z, den[3])));
-    if (!(D != 0.0) || !(fabs(N) < 1e300)) return -1;
-    const double h = frac > 0.f ? (double)i + 0.5 : (double)i - 0.5;
-    const double e = fma(-h, D, N);  // (N/D - h) * D
-    if (frac > 0.f) return (D > 0.0 ? e >= 0.0 : e <= 0.0) ? i + 1 : i;
-    return (D > 0.0 ? e < 0.0 : e > 0.0) ? i - 1 : i;
-}
-
-// Bilinear rule of get_bilinear_interp (CB_backproject.cu:221-254), same
-// operation order.
-__device__ __forceinline__ float fetch_bilinear(const BPParams &P, const float *pvw, float fu, float fv) {
-    if (fu <= -1.f || fv <= -1.f || fu >= (float)P.nu || fv >= (float)P.nv) return 0.f;
-    const int i0 = (int)floorf(fu), j0 = (int)floorf(fv);
-    const float fx = fu - (float)i0, fy = fv - (float)j0;
-    auto get = [&](int i, int j) -> float {
-        if (i < 0 || i >= (int)P.nu || j < 0 || j >= (int)P.nv) return 0.f;
-        return __ldg(pvw + (i * P.su + j * P.sv));
-    };
-    const float v00 = get(i0, j0), v01 = get(i0, j0 + 1), v10 = get(i0 + 1, j0), v11 = get(i0 + 1, j0 + 1);
-    const float t1 = v00 * (1.f - fx) + v10 * fx;
-    const float t2 = v01 * (1.f - fx) + v11 * fx;
-    return t1 * (1.f - fy) + t2 * fy;
-}
-
-__device__ __forceinline__ float dot4(const float4 a, float x, float y, float z) {
-    return fmaf(a.x, x, fmaf(a.y, y, fmaf(a.z, z, a.w)));
-}
-
-// 1/x with one MUFU op (relative error < 2^-22); nearest-pixel ties are
-// settled in FP64 separately.
-__device__ __forceinline__ float rcp_fast(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
-__device__ __forceinline__ float taper(const ab_bpview &b, float fu, float fv, float inv_sep) {
-    if (fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv) return 1.f;
-    return ab_edge_taper(fu - b.cu0, fv - b.cv0, b.inv_halfu, b.inv_halfv, inv_sep);
-}
-
-__device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, float Z) {
-    float w = 1.f;
-    if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
-    if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
-    return w;
-}
-
-// EXACT: chord-length footprint (CB_backproject.cu:408-477).
-// RAYCAST: fast mode with direct-raycast weights (:512-646, preset 0).
-// BILIN: bilinear instead of nearest detector sampling.
-// ORD: 0 = C order (fastest axis z, slowest x), 1 = F order (fastest x).
-// XB: voxels per thread along the slowest axis (4: more reuse of each view's
-// coefficients, 2: fewer registers and more resident warps).
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
-__global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(BPParams P) {
-    constexpr int kXB = XB;
-    constexpr bool kNear = !EXACT && !BILIN;
-    __shared__ ab_bpview sv[kChunk];
-    __shared__ ab_bpview_d svd[kNear ? kChunk : 1];
-    __shared__ ab_bpview_exact sx[EXACT ? kChunk : 1];
-
-    // Brick-ordered block coordinates (uniform per CTA).
-    const int per_sb = P.gb[0] * P.sb1 * P.sb2;
-    const int sb = blockIdx.x / per_sb;
-    int r = blockIdx.x - sb * per_sb;
-    const int b0 = r % P.gb[0];
-    r /= P.gb[0];
-    const int b1 = (sb % P.nsb1) * P.sb1 + r % P.sb1;
-    const int b2 = (sb / P.nsb1) * P.sb2 + r / P.sb1;
-    if (b1 >= P.gb[1] || b2 >= P.gb[2]) return;  // the whole CTA exits before any barrier
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i0 = b0 * 32 + lane;
-    const int i1 = b1 * 8 + warp;
-    const int i2b = b2 * kXB;
-    constexpr int a0 = ORD == 0 ? 2 : 0, a1 = 1, a2 = ORD == 0 ? 0 : 2;
-    const bool in01 = i0 < P.n[a0] && i1 < P.n[a1];
-
-    // Voxel-centre coordinates relative to the volume centre, per axis.
-    const float vw = P.voxwid;
-    float base[3];
-    int idx[3];
-    idx[a0] = i0;
-    idx[a1] = i1;
-    idx[a2] = i2b;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) base[a] = ((float)idx[a] + 0.5f - 0.5f * (float)P.n[a]) * vw;
-
-    // Cylinder mask about world x = y = 0 (CB_backproject.cu:339-343).
-    bool live[kXB];
-    bool any_live = false;
-#pragma unroll
-    for (int k = 0; k < kXB; ++k) {
-        float c[3] = {base[0], base[1], base[2]};
-        c[a2] += (float)k * vw;
-        bool ok = in01 && (i2b + k) < P.n[a2];
-        if (ok && P.mask) {
-            const float xw = c[0] + P.c0[0], yw = c[1] + P.c0[1];
-            ok = !(xw * xw + yw * yw > P.mask_r2);
-        }
-        live[k] = ok;
-        any_live |= ok;
-    }
-
-    // One accumulator per voxel over all views and sub-samples; the mean over
-    // the ssx*ssy*ssz sub-samples is taken at the end (the reference averages
-    // level by level, CB_backproject.cu:717-731 -- the same value up to float
-    // rounding, identical when there is no supersampling).
-    float acc[kXB];
-#pragma unroll
-    for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
-
-    const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
-    const bool needZ = P.pL != 0 || P.pV != 0;
-    const int n_sub = P.ssx * P.ssy * P.ssz;
-    for (int isub = 0; isub < n_sub; ++isub) {
-        const int si = isub / (P.ssy * P.ssz), sj = (isub / P.ssz) % P.ssy, sk = isub % P.ssz;
-        {
-            {
-                const float fsub[3] = {-0.5f + offx * (0.5f + si), -0.5f + offy * (0.5f + sj),
-                                       -0.5f + offz * (0.5f + sk)};
-                const float X0 = base[0] + fsub[0] * vw, Y0 = base[1] + fsub[1] * vw, Z0 = base[2] + fsub[2] * vw;
-
-                for (uint32_t v0 = 0; v0 < P.n_views; v0 += kChunk) {
-                    const int cn = (int)min((uint32_t)kChunk, P.n_views - v0);
-                    __syncthreads();
-                    for (int t = threadIdx.x; t < cn; t += kThreads) {
-                        // Volume centre in FP64 (exact: corner and voxwid are floats, n an integer).
-                        const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
-                                        P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
-                        const aprict_proj_spec sp = P.specs[v0 + t];
-                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t], kNear ? &svd[t] : nullptr) && P.status)
-                            atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
-                        if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
-                    }
-                    __syncthreads();
-                    if (!any_live) continue;
-                    for (int t = 0; t < cn; ++t) {
-                        const int view = (int)v0 + t;
-                        const ab_bpview b = sv[t];
-                        const float *pvw = P.projs + (int64_t)view * P.stride_view;
-                        const float Nu0 = dot4(b.nu, X0, Y0, Z0), Nv0 = dot4(b.nv, X0, Y0, Z0);
-                        const float D0 = dot4(b.den, X0, Y0, Z0);
-                        const float dNu = (a2 == 0 ? b.nu.x : (a2 == 1 ? b.nu.y : b.nu.z)) * vw;
-                        const float dNv = (a2 == 0 ? b.nv.x : (a2 == 1 ? b.nv.y : b.nv.z)) * vw;
-                        const float dD = (a2 == 0 ? b.den.x : (a2 == 1 ? b.den.y : b.den.z)) * vw;
-                        float Zb = 0.f, dZ = 0.f;
-                        if (needZ) {
-                            Zb = dot4(b.zl, X0, Y0, Z0);
-                            dZ = (a2 == 0 ? b.zl.x : (a2 == 1 ? b.zl.y : b.zl.z)) * vw;
-                        }
-                        if constexpr (EXACT) {
-#pragma unroll
-                            for (int k = 0; k < kXB; ++k) {
-                                if (!live[k]) continue;
-                                const float kf = (float)k;
-                                const float D = fmaf(kf, dD, D0);
-                                const float rD = rcp_fast(D);
-                                const float fu = fmaf(kf, dNu, Nu0) * rD;
-                                const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                float s;
-                                {
-                                    // Footprint: bounding box of the 8 projected corners.
-                                    const ab_bpview_exact e = sx[t];
-                                    const float h = 0.5f * vw;
-                                    const float hu[3] = {b.nu.x * h, b.nu.y * h, b.nu.z * h};
-                                    const float hv[3] = {b.nv.x * h, b.nv.y * h, b.nv.z * h};
-                                    const float hd[3] = {b.den.x * h, b.den.y * h, b.den.z * h};
-                                    const float Nu = fmaf(kf, dNu, Nu0), Nv = fmaf(kf, dNv, Nv0);
-                                    float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
-#pragma unroll
-                                    for (int c = 0; c < 8; ++c) {
-                                        const float sx_ = (c & 4) ? 1.f : -1.f, sy_ = (c & 2) ? 1.f : -1.f,
-                                                    sz_ = (c & 1) ? 1.f : -1.f;
-                                        const float dd = D + sx_ * hd[0] + sy_ * hd[1] + sz_ * hd[2];
-                                        const float rr = rcp_fast(dd);
-                                        const float uu = (Nu + sx_ * hu[0] + sy_ * hu[1] + sz_ * hu[2]) * rr;
-                                        const float vv = (Nv + sx_ * hv[0] + sy_ * hv[1] + sz_ * hv[2]) * rr;
-                                        umin = fminf(umin, uu);
-                                        umax = fmaxf(umax, uu);
-                                        vmin = fminf(vmin, vv);
-                                        vmax = fmaxf(vmax, vv);
-                                    }
-                                    const int ulo = max(0, (int)ceilf(umin - 1e-3f));
-                                    const int uhi = min((int)P.nu - 1, (int)floorf(umax + 1e-3f));
-                                    const int vlo = max(0, (int)ceilf(vmin - 1e-3f));
-                                    const int vhi = min((int)P.nv - 1, (int)floorf(vmax + 1e-3f));
-                                    // Ray origin relative to this voxel's centre.
-                                    float cx[3] = {X0, Y0, Z0};
-                                    cx[a2] += kf * vw;
-                                    const float r0x = e.s.x - cx[0], r0y = e.s.y - cx[1], r0z = e.s.z - cx[2];
-                                    s = 0.f;
-                                    for (int iu = ulo; iu <= uhi; ++iu) {
-                                        const float dux = fmaf(e.u.x, (float)iu, e.d0.x);
-                                        const float duy = fmaf(e.u.y, (float)iu, e.d0.y);
-                                        const float duz = fmaf(e.u.z, (float)iu, e.d0.z);
-                                        for (int iv = vlo; iv <= vhi; ++iv) {
-                                            const float dx = fmaf(e.v.x, (float)iv, dux);
-                                            const float dy = fmaf(e.v.y, (float)iv, duy);
-                                            const float dz = fmaf(e.v.z, (float)iv, duz);
-                                            float a_lo = 0.f, a_hi = 3.0e38f;
-                                            bool miss = false;
-                                            if (dx != 0.f) {
-                                                const float inv = rcp_fast(dx);
-                                                const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
-                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                            } else {
-                                                miss |= fabsf(r0x) > h;
-                                            }
-                                            if (dy != 0.f) {
-                                                const float inv = rcp_fast(dy);
-                                                const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
-                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                            } else {
-                                                miss |= fabsf(r0y) > h;
-                                            }
-                                            if (dz != 0.f) {
-                                                const float inv = rcp_fast(dz);
-                                                const float t1 = (-h - r0z) * inv, t2 = (h - r0z) * inv;
-                                                a_lo = fmaxf(a_lo, fminf(t1, t2));
-                                                a_hi = fminf(a_hi, fmaxf(t1, t2));
-                                            } else {
-                                                miss |= fabsf(r0z) > h;
-                                            }
-                                            if (miss || !(a_hi > a_lo)) continue;
-                                            const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
-                                            const float pv = P.all_ones ? 1.f : __ldg(pvw + (iu * P.su + iv * P.sv));
-                                            s = fmaf(pv, chord, s);
-                                        }
-                                    }
-                                    if (needZ) s *= zpow(P, b, fmaf(kf, dZ, Zb));
-                                }
-                                if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
-                                acc[k] += s;
-                            }
-                        } else {
-                            // Fast modes: one branch-free pass over the thread's voxels;
-                            // voxel-views that need more (a near-tie pixel choice, the
-                            // detector-edge taper band) are flagged and finished in a rare
-                            // second pass, so the common path has no divergent branches.
-                            unsigned pending = 0;
-#pragma unroll
-                            for (int k = 0; k < kXB; ++k) {
-                                const float kf = (float)k;
-                                const float D = fmaf(kf, dD, D0);
-                                const float rD = rcp_fast(D);
-                                const float fu = fmaf(kf, dNu, Nu0) * rD;
-                                const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                float w = RAYCAST ? 1.f : b.kfast * rD * rD;
-                                if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
-                                // inner: inside the taper's flat box, which lies inside the
-                                // detector (|f - c| <= n/2 without a taper)
-                                const bool inner = fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv;
-                                float pv = 0.f;
-                                bool fast;
-                                if (BILIN) {
-                                    fast = inner;
-                                    pv = fetch_bilinear(P, pvw, fu, fv);
-                                    pv = live[k] && fast ? pv : 0.f;
-                                } else {
-                                    // Inside the detector box |f| < 2^22, so the rounding trick
-                                    // needs no clamp; a pixel at most 1/2 - refine from f is
-                                    // then a valid index (the box edges are half-integers).
-                                    const float tu = __fadd_rn(fu, kMagic), tv = __fadd_rn(fv, kMagic);
-                                    const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
-                                    const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
-                                    fast = inner && fabsf(du) <= P.tie && fabsf(dv) <= P.tie;
-                                    // pixel offset from the rounded indices (bits - magic)
-                                    const int off = (__float_as_int(tu) - 0x4B400000) * P.su + (__float_as_int(tv) - 0x4B400000) * P.sv;
-                                    if (live[k] && fast) pv = __ldg(pvw + off);
-                                }
-                                acc[k] = fmaf(pv, w, acc[k]);
-                                pending |= (live[k] && !fast) ? 1u << k : 0u;
-                            }
-                            if (pending != 0u) {
-#pragma unroll
-                                for (int k = 0; k < kXB; ++k) {
-                                    if (!((pending >> k) & 1u)) continue;
-                                    const float kf = (float)k;
-                                    const float D = fmaf(kf, dD, D0);
-                                    const float rD = rcp_fast(D);
-                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
-                                    const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                    float w = RAYCAST ? 1.f : b.kfast * rD * rD;
-                                    if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
-                                    float pv;
-                                    if (BILIN) {
-                                        pv = fetch_bilinear(P, pvw, fu, fv);
-                                    } else {
-                                        float du, dv;
-                                        int iu = round_index(fu, -2.f, P.fnu1, du);
-                                        int iv = round_index(fv, -2.f, P.fnv1, dv);
-                                        const bool tu = fabsf(du) > P.tie, tv = fabsf(dv) > P.tie;
-                                        if (tu || tv) {
-                                            int id[3];
-                                            id[a0] = i0;
-                                            id[a1] = i1;
-                                            id[a2] = i2b + k;
-                                            const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
-                                                            ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
-                                                            ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
-                                            const ab_bpview_d &c = svd[kNear ? t : 0];
-                                            if (tu) iu = refine_index(c.nu, c.den, vr, iu, du);
-                                            if (tv) iv = refine_index(c.nv, c.den, vr, iv, dv);
-                                        }
-                                        const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
-                                        pv = inb ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
-                                    }
-                                    float s = pv * w;
-                                    if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
-                                    acc[k] += s;
-                                }
-                            }
-                        }
-                    }
-                }
-            }
-        }
-    }
-
-#pragma unroll
-    for (int k = 0; k < kXB; ++k) {
-        if (!live[k]) continue;
-        const float value = n_sub == 1 ? acc[k] : acc[k] / (float)n_sub;
-        if (value == 0.f) continue;  // the reference skips the write (:1010)
-        int id[3];
-        id[a0] = i0;
-        id[a1] = i1;
-        id[a2] = i2b + k;
-        const int64_t o = (int64_t)id[0] * P.vs[0] + (int64_t)id[1] * P.vs[1] + (int64_t)id[2] * P.vs[2];
-        const float m = P.mult ? __ldcs(P.mult + o) : 1.f;
-        __stcs(P.vol + o, value * m + __ldcs(P.vol + o));
-    }
+__global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(const BPParams P) {
+    __shared__ BPSmem<EXACT, BILIN> sm;
+    bp_brick<ORD, EXACT, RAYCAST, BILIN, XB>(P, blockIdx.x, sm);
 }
 
 template <int ORD, int XB>
@@ -453,103 +37,11 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
                                        const float *projs_dev, const aprict_vol_desc *vd, float *vol_dev,
                                        const float *multiplier_dev, const aprict_backproject_config *cfg,
                                        uint32_t *status_dev, aprict_stream_t stream) {
-    int rc;
-    if ((rc = ab_check_projs(pd, projs_dev, "projections")) != APRICT_OK) return rc;
-    if ((rc = ab_check_vol(vd, vol_dev, "volume")) != APRICT_OK) return rc;
-    if (cfg == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null backproject config");
-    if (cfg->apply_summand_multiplier != (multiplier_dev != nullptr ? 1u : 0u))
-        return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
-                       "apply_summand_multiplier must be set if and only if a multiplier is given");
-    if (cfg->weighting_preset != 0)
-        return ab_fail(APRICT_ERR_UNSUPPORTED, "backprojection weighting preset %u is not implemented",
-                       cfg->weighting_preset);
-    if (cfg->ssx == 0 || cfg->ssy == 0 || cfg->ssz == 0 || cfg->ssx > 16 || cfg->ssy > 16 || cfg->ssz > 16)
-        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ssx/ssy/ssz must be in [1, 16]");
-    if (cfg->Z_on_val_factor_power != 0 && !(cfg->Z_on_val_factor_val != 0.f))
-        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "Z_on_val_factor_val must be nonzero");
-    if (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) return APRICT_OK;
-    if (specs_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null view specs");
-    if (multiplier_dev && (reinterpret_cast<uintptr_t>(multiplier_dev) & 3u))
-        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "multiplier pointer not 4-byte aligned");
-    if (pd->nu > (1u << 21) || pd->nv > (1u << 21))
-        return ab_fail(APRICT_ERR_TOO_LARGE, "backprojection supports at most 2^21 detector pixels per axis");
-    if ((int64_t)(pd->nu - 1) * pd->stride_u + (int64_t)(pd->nv - 1) * pd->stride_v + 1 > 0x7fffffffLL)
-        return ab_fail(APRICT_ERR_TOO_LARGE, "one projection image spans more than 2^31 elements");
-
-    BPParams P{};
-    P.specs = specs_dev;
-    P.n_views = pd->n_views;
-    P.nu = pd->nu;
-    P.nv = pd->nv;
-    P.stride_view = pd->stride_view;
-    P.su = (int)pd->stride_u;
-    P.sv = (int)pd->stride_v;
-    P.fnu1 = (float)pd->nu + 1.f;
-    P.fnv1 = (float)pd->nv + 1.f;
-    P.tie = 0.5f - 2e-3f * fmaxf(1.f, (float)(pd->nu > pd->nv ? pd->nu : pd->nv) / 1024.f);
-    P.projs = projs_dev;
-    P.vol = vol_dev;
-    P.mult = multiplier_dev;
-    P.n[0] = (int)vd->nx;
-    P.n[1] = (int)vd->ny;
-    P.n[2] = (int)vd->nz;
-    if (vd->order == 0) {
-        P.vs[0] = (int64_t)vd->ny * vd->nz;
-        P.vs[1] = vd->nz;
-        P.vs[2] = 1;
-    } else {
-        P.vs[0] = 1;
-        P.vs[1] = vd->nx;
-        P.vs[2] = (int64_t)vd->nx * vd->ny;
-    }
-    P.voxwid = vd->voxwid;
-    P.vwd = (double)vd->voxwid;
-    P.cornerd[0] = vd->corner.x;
-    P.cornerd[1] = vd->corner.y;
-    P.cornerd[2] = vd->corner.z;
-    P.c0[0] = vd->corner.x + 0.5f * vd->voxwid * (float)vd->nx;
-    P.c0[1] = vd->corner.y + 0.5f * vd->voxwid * (float)vd->ny;
-    P.c0[2] = vd->corner.z + 0.5f * vd->voxwid * (float)vd->nz;
-    P.mask = cfg->mask_to_cylinder ? 1 : 0;
-    P.mask_r2 = cfg->mask_to_cyl_rad * cfg->mask_to_cyl_rad;
-    P.all_ones = cfg->backproject_all_1s ? 1 : 0;
-    P.sep = cfg->soften_edge_proportion;
-    P.inv_sep = P.sep > 0.f ? 1.f / P.sep : 0.f;
-    P.pL = cfg->Z_on_L_factor_power;
-    P.pV = cfg->Z_on_val_factor_power;
-    P.val = cfg->Z_on_val_factor_val;
-    P.ssx = (int)cfg->ssx;
-    P.ssy = (int)cfg->ssy;
-    P.ssz = (int)cfg->ssz;
-    P.status = status_dev;
-
-    const int xb = ab_tuning_get(AB_TUNE_BP_XB) == 4 ? 4 : 2;
-    const int kXB = xb;
-    const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
-    P.gb[0] = (n0 + 31) / 32;
-    P.gb[1] = (n1 + 7) / 8;
-    P.gb[2] = (n2 + kXB - 1) / kXB;
-    // Super-brick: all blocks of the fastest axis x sb1 x sb2 blocks (8 and
-    // kXB voxels each), about one wave of resident CTAs, with equal extents in
-    // voxels along the middle and slowest axes.
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-    }
-    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : 3;
-    const double target = (double)wave * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
-    int sb1 = (int)floor(sqrt(target * kXB / 8.0) + 0.5);
-    sb1 = sb1 < 1 ? 1 : (sb1 > P.gb[1] ? P.gb[1] : sb1);
-    int sb2 = (int)floor(target / sb1 + 0.5);
-    sb2 = sb2 < 1 ? 1 : (sb2 > P.gb[2] ? P.gb[2] : sb2);
-    P.sb1 = sb1;
-    P.sb2 = sb2;
-    P.nsb1 = (P.gb[1] + sb1 - 1) / sb1;
-    const int64_t nsb = (int64_t)P.nsb1 * ((P.gb[2] + sb2 - 1) / sb2);
-    const int64_t grid = nsb * P.gb[0] * sb1 * sb2;
-    if (grid > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
+    BPParams P;
+    uint64_t grid = 0;
+    int xb = 2;
+    const int rc = make_bp_params(specs_dev, pd, projs_dev, vd, vol_dev, multiplier_dev, cfg, status_dev, P, grid, xb);
+    if (rc != APRICT_OK || grid == 0) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const bool lin = cfg->approx_mode_linear_interpolate != 0;
     if (xb == 4) {

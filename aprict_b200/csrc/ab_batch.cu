@@ -1,0 +1,371 @@
+// ab_batch.cu -- many independent scans in one persistent launch.
+//
+// The reference projects and backprojects one scan per call, each call a
+// sequence of launches sized to that scan (flatpanel.py:1047-1122,
+// 1161-1278); a workload of many small, uneven scans leaves most of the GPU
+// idle at the tail of every launch and pays a launch and a host
+// synchronisation per 10 views. Here a batch of scans is one plan: the
+// per-scan parameters of the one-scan kernels (FPScan / BPParams) plus the
+// prefix sums of their work-unit counts. One persistent launch of
+// (SMs x resident CTAs) CTAs then pulls work units from a global counter --
+// the detector tiles of every scan for a projection, the volume bricks of
+// every scan for a backprojection -- so the whole GPU stays busy across scan
+// boundaries. Scans are ordered largest first so that the small ones fill the
+// tail. The counter lives in the plan; the last CTA to finish puts it back to
+// zero, so a plan is relaunched (or replayed in a CUDA graph) with no host
+// work. There are no waits between CTAs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "ab_bpbrick.cuh"
+#include "ab_fptile.cuh"
+
+namespace {
+
+constexpr uint32_t kPlanMagic = 0x41424232u;  // "ABB2"
+constexpr int kGroup = 96;                    // scans per launch (kernel-parameter space)
+
+// Plan layout (host image; the caller's device copy is used only for the
+// per-group counters): header, then n_groups Group records (256 bytes
+// apart, so each group's counters own their line), then the per-scan
+// parameters in execution order.
+struct PlanHeader {
+    uint32_t magic;
+    int32_t op;       // APRICT_BATCH_PROJECT / APRICT_BATCH_BACKPROJECT
+    int32_t n_scans;
+    int32_t variant;  // kernel template variant (see the run function)
+    int32_t n_groups;
+    int32_t pad_;
+    uint64_t groups_off, params_off, bytes;
+};
+
+struct Group {
+    uint32_t counter;  // next work unit; zero between launches (device copy)
+    uint32_t exited;   // CTAs finished in the current launch; zero between launches
+    uint32_t first;    // first scan (execution order)
+    uint32_t count;    // scans in the group
+    uint32_t n_units;
+    int32_t grid;                 // persistent CTAs (SMs x resident CTAs, at most n_units)
+    uint32_t prefix[kGroup + 1];  // cumulative work units of the group's scans
+};
+
+// Launch arguments: the group's scans travel in the kernel parameter space
+// (constant bank), where the per-scan fields cost no registers to keep.
+template <class Params>
+struct BatchArgs {
+    Group *g;  // device copy of the group record (counters)
+    uint32_t count, n_units;
+    uint32_t prefix[kGroup + 1];
+    Params scans[kGroup];
+};
+static_assert(sizeof(BatchArgs<ab_bp::BPParams>) <= 32000, "batch arguments exceed the kernel parameter space");
+static_assert(sizeof(BatchArgs<ab_fp::FPScan<int64_t>>) <= 32000, "batch arguments exceed the kernel parameter space");
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t params_size(int op) {
+    return op == APRICT_BATCH_PROJECT ? std::max(sizeof(ab_fp::FPScan<int64_t>), sizeof(ab_fp::FPScan<int32_t>))
+                                      : sizeof(ab_bp::BPParams);
+}
+
+int n_groups_of(int n) { return (n + kGroup - 1) / kGroup; }
+
+size_t plan_bytes(int op, int n) {
+    return align256(sizeof(PlanHeader)) + (size_t)n_groups_of(n) * align256(sizeof(Group)) +
+           align256(params_size(op) * (size_t)n);
+}
+
+// Work-unit fetch shared by both kernels: thread 0 takes the next unit and
+// finds its scan (binary search over the prefix sums); the CTA reads both
+// from shared memory. Returns false when the group is exhausted.
+template <class Args>
+__device__ __forceinline__ bool next_unit(const Args &A, uint32_t &unit, int &scan) {
+    __shared__ uint32_t s_unit;
+    __shared__ int s_scan;
+    if (threadIdx.x == 0) {
+        const uint32_t it = atomicAdd(&A.g->counter, 1u);
+        int s = 0;
+        if (it < A.n_units) {
+            int lo = 0, hi = (int)A.count - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (A.prefix[mid] <= it)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            s = lo;
+        }
+        s_unit = it;
+        s_scan = s;
+    }
+    __syncthreads();
+    unit = s_unit;
+    scan = s_scan;
+    __syncthreads();  // s_unit is rewritten only after every thread has read it
+    if (unit >= A.n_units) return false;
+    unit -= A.prefix[scan];
+    return true;
+}
+
+// The last CTA of a launch puts the counters back to zero for the next one.
+// Every CTA has taken its final (out-of-range) unit before it counts itself
+// out, so no unit is fetched after the reset.
+__device__ __forceinline__ void retire(Group *g) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&g->exited, 1u) + 1u;
+        if (done == gridDim.x) {
+            g->counter = 0u;
+            g->exited = 0u;
+            __threadfence();
+        }
+    }
+}
+
+template <typename Off>
+__global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __grid_constant__ BatchArgs<ab_fp::FPScan<Off>> A) {
+    uint32_t unit;
+    int s;
+    while (next_unit(A, unit, s)) ab_fp::fp_tile(A.scans[s], unit);
+    retire(A.g);
+}
+
+template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
+__global__ void __launch_bounds__(ab_bp::kThreads, 3) k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
+    __shared__ ab_bp::BPSmem<EXACT, BILIN> sm;
+    uint32_t unit;
+    int s;
+    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, 2>(A.scans[s], unit, sm);
+    retire(A.g);
+}
+
+// Backprojection kernel variant code: ORD | mode << 1, mode 0 fast nearest,
+// 1 fast bilinear, 2 raycast nearest, 3 raycast bilinear, 4 exact.
+int bp_variant(const aprict_backproject_config *c, uint32_t order) {
+    const int mode = c->exact ? 4
+                              : (c->approx_mode_direct_raycast ? 2 : 0) + (c->approx_mode_linear_interpolate ? 1 : 0);
+    return (int)order | (mode << 1);
+}
+
+int sm_count(int &sms) {
+    static int cached = 0;
+    if (cached == 0) {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            return ab_fail(APRICT_ERR_CUDA, "cannot query the multiprocessor count");
+        cached = n;
+    }
+    sms = cached;
+    return APRICT_OK;
+}
+
+// Persistent grid of a kernel: SMs x resident CTAs (the query also loads the
+// kernel, so a later launch inside a stream capture loads nothing).
+template <class K>
+int grid_for(K kernel, uint32_t n_units, int32_t &grid) {
+    int sms = 0, per_sm = 0;
+    const int rc = sm_count(sms);
+    if (rc != APRICT_OK) return rc;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0) != cudaSuccess || per_sm <= 0)
+        return ab_fail(APRICT_ERR_CUDA, "occupancy query failed");
+    grid = (int32_t)std::min<uint64_t>((uint64_t)sms * per_sm, n_units);
+    return APRICT_OK;
+}
+
+template <class Params, class K>
+int launch_group(K kernel, const PlanHeader *H, const Group &gh, Group *gd, const char *params_host,
+                 cudaStream_t st) {
+    if (gh.n_units == 0) return APRICT_OK;
+    const int grid = gh.grid;
+    if (grid <= 0) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (grid)");
+    BatchArgs<Params> A;
+    A.g = gd;
+    A.count = gh.count;
+    A.n_units = gh.n_units;
+    memcpy(A.prefix, gh.prefix, sizeof(A.prefix));
+    memcpy(A.scans, params_host + (size_t)gh.first * sizeof(Params), sizeof(Params) * gh.count);
+    (void)H;
+    kernel<<<grid, 256, 0, st>>>(A);
+    return ab_cuda_check(cudaGetLastError(), "batch launch");
+}
+
+int scan_error(int rc, int i) {
+    char msg[512];
+    snprintf(msg, sizeof(msg), "%s", aprict_b200_last_error());
+    return ab_fail(rc, "scan %d: %s", i, msg);
+}
+
+}  // namespace
+
+extern "C" size_t aprict_b200_batch_plan_bytes(int op, int n_scans) {
+    if ((op != APRICT_BATCH_PROJECT && op != APRICT_BATCH_BACKPROJECT) || n_scans <= 0) return 0;
+    return plan_bytes(op, n_scans);
+}
+
+extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_scans, const void *configs,
+                                      void *plan_host, size_t plan_capacity) {
+    if (op != APRICT_BATCH_PROJECT && op != APRICT_BATCH_BACKPROJECT)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "unknown batch operation %d", op);
+    if (scans == nullptr || configs == nullptr || plan_host == nullptr || n_scans <= 0)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "batch plan needs scans, configs and a plan buffer");
+    const size_t need = plan_bytes(op, n_scans);
+    if (plan_capacity < need)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "plan buffer too small: %zu bytes, %zu needed", plan_capacity,
+                       need);
+    if (reinterpret_cast<uintptr_t>(plan_host) & 255u)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "plan buffer must be 256-byte aligned");
+
+    // Validate every scan and build its parameters with the one-scan code.
+    std::vector<uint64_t> units(n_scans, 0);
+    std::vector<ab_fp::FPScan<int32_t>> fp32(op == APRICT_BATCH_PROJECT ? n_scans : 0);
+    std::vector<ab_fp::FPScan<int64_t>> fp64(op == APRICT_BATCH_PROJECT ? n_scans : 0);
+    std::vector<ab_bp::BPParams> bp(op == APRICT_BATCH_BACKPROJECT ? n_scans : 0);
+    bool all_small = true;
+    int variant = -1;
+    for (int i = 0; i < n_scans; ++i) {
+        const aprict_scan &sc = scans[i];
+        int rc;
+        if (op == APRICT_BATCH_PROJECT) {
+            const aprict_project_config *cfg = static_cast<const aprict_project_config *>(configs) + i;
+            rc = ab_fp::fp_check(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, cfg);
+            if (rc != APRICT_OK) return scan_error(rc, i);
+            all_small = all_small && ab_fp::small_volume(&sc.vol);
+            uint64_t u = 0;
+            fp32[i] = ab_fp::make_fpscan<int32_t>(sc.specs_dev, &sc.projs, sc.projs_dev, sc.base_dev, &sc.vol,
+                                                  sc.vol_dev, cfg, sc.status_dev, u);
+            fp64[i] = ab_fp::make_fpscan<int64_t>(sc.specs_dev, &sc.projs, sc.projs_dev, sc.base_dev, &sc.vol,
+                                                  sc.vol_dev, cfg, sc.status_dev, u);
+            units[i] = u;
+        } else {
+            const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
+            int xb = 2;
+            uint64_t u = 0;
+            // The batch kernel carries two voxels per thread.
+            rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
+                                       cfg, sc.status_dev, bp[i], u, xb, 2);
+            if (rc != APRICT_OK) return scan_error(rc, i);
+            const int v = bp_variant(cfg, sc.vol.order);
+            if (variant >= 0 && v != variant)
+                return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
+                               "scan %d: every scan of a backprojection batch needs the same volume order and "
+                               "backprojection mode (exact / fast / raycast, nearest / bilinear)",
+                               i);
+            variant = v;
+            units[i] = u;
+        }
+    }
+    if (op == APRICT_BATCH_PROJECT) variant = all_small ? 0 : 1;
+
+    // Largest scans first; zero-unit scans are kept (they take no units).
+    std::vector<int> order(n_scans);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return units[a] > units[b]; });
+
+    char *base = static_cast<char *>(plan_host);
+    memset(base, 0, need);
+    PlanHeader *H = reinterpret_cast<PlanHeader *>(base);
+    H->magic = kPlanMagic;
+    H->op = op;
+    H->n_scans = n_scans;
+    H->variant = variant;
+    H->n_groups = n_groups_of(n_scans);
+    H->groups_off = align256(sizeof(PlanHeader));
+    H->params_off = H->groups_off + (size_t)H->n_groups * align256(sizeof(Group));
+    H->bytes = need;
+    for (int gi = 0; gi < H->n_groups; ++gi) {
+        Group *G = reinterpret_cast<Group *>(base + H->groups_off + (size_t)gi * align256(sizeof(Group)));
+        G->first = (uint32_t)(gi * kGroup);
+        G->count = (uint32_t)std::min(kGroup, n_scans - gi * kGroup);
+        uint64_t acc = 0;
+        for (uint32_t k = 0; k < G->count; ++k) {
+            G->prefix[k] = (uint32_t)acc;
+            acc += units[order[G->first + k]];
+        }
+        for (uint32_t k = G->count; k <= (uint32_t)kGroup; ++k) G->prefix[k] = (uint32_t)acc;
+        if (acc >= 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "batch has too many work units");
+        G->n_units = (uint32_t)acc;
+        int rc = APRICT_OK;
+        if (G->n_units > 0) {
+            if (op == APRICT_BATCH_PROJECT) {
+                rc = variant == 0 ? grid_for(k_batch_project<int32_t>, G->n_units, G->grid)
+                                  : grid_for(k_batch_project<int64_t>, G->n_units, G->grid);
+            } else {
+                switch (variant) {
+                    case 0: rc = grid_for(k_batch_backproject<0, false, false, false>, G->n_units, G->grid); break;
+                    case 1: rc = grid_for(k_batch_backproject<1, false, false, false>, G->n_units, G->grid); break;
+                    case 2: rc = grid_for(k_batch_backproject<0, false, false, true>, G->n_units, G->grid); break;
+                    case 3: rc = grid_for(k_batch_backproject<1, false, false, true>, G->n_units, G->grid); break;
+                    case 4: rc = grid_for(k_batch_backproject<0, false, true, false>, G->n_units, G->grid); break;
+                    case 5: rc = grid_for(k_batch_backproject<1, false, true, false>, G->n_units, G->grid); break;
+                    case 6: rc = grid_for(k_batch_backproject<0, false, true, true>, G->n_units, G->grid); break;
+                    case 7: rc = grid_for(k_batch_backproject<1, false, true, true>, G->n_units, G->grid); break;
+                    case 8: rc = grid_for(k_batch_backproject<0, true, false, false>, G->n_units, G->grid); break;
+                    case 9: rc = grid_for(k_batch_backproject<1, true, false, false>, G->n_units, G->grid); break;
+                    default: rc = ab_fail(APRICT_ERR_INVALID_ARGUMENT, "unsupported backprojection mode");
+                }
+            }
+        }
+        if (rc != APRICT_OK) return rc;
+    }
+    char *params = base + H->params_off;
+    for (int k = 0; k < n_scans; ++k) {
+        const int i = order[k];
+        if (op == APRICT_BATCH_PROJECT) {
+            if (variant == 0)
+                memcpy(params + k * sizeof(ab_fp::FPScan<int32_t>), &fp32[i], sizeof(ab_fp::FPScan<int32_t>));
+            else
+                memcpy(params + k * sizeof(ab_fp::FPScan<int64_t>), &fp64[i], sizeof(ab_fp::FPScan<int64_t>));
+        } else {
+            memcpy(params + k * sizeof(ab_bp::BPParams), &bp[i], sizeof(ab_bp::BPParams));
+        }
+    }
+    return APRICT_OK;
+}
+
+extern "C" int aprict_b200_batch_run(const void *plan_host, void *plan_dev, aprict_stream_t stream) {
+    if (plan_host == nullptr || plan_dev == nullptr)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "batch run needs the host plan and its device copy");
+    if (reinterpret_cast<uintptr_t>(plan_dev) & 255u)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "device plan must be 256-byte aligned");
+    const PlanHeader *H = static_cast<const PlanHeader *>(plan_host);
+    if (H->magic != kPlanMagic) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "not a batch plan");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const char *hb = static_cast<const char *>(plan_host);
+    char *db = static_cast<char *>(plan_dev);
+    const char *params = hb + H->params_off;
+    for (int gi = 0; gi < H->n_groups; ++gi) {
+        const size_t off = H->groups_off + (size_t)gi * align256(sizeof(Group));
+        const Group &gh = *reinterpret_cast<const Group *>(hb + off);
+        Group *gd = reinterpret_cast<Group *>(db + off);
+        int rc;
+        if (H->op == APRICT_BATCH_PROJECT) {
+            rc = H->variant == 0
+                     ? launch_group<ab_fp::FPScan<int32_t>>(k_batch_project<int32_t>, H, gh, gd, params, st)
+                     : launch_group<ab_fp::FPScan<int64_t>>(k_batch_project<int64_t>, H, gh, gd, params, st);
+        } else {
+            using BP = ab_bp::BPParams;
+            switch (H->variant) {
+                case 0: rc = launch_group<BP>(k_batch_backproject<0, false, false, false>, H, gh, gd, params, st); break;
+                case 1: rc = launch_group<BP>(k_batch_backproject<1, false, false, false>, H, gh, gd, params, st); break;
+                case 2: rc = launch_group<BP>(k_batch_backproject<0, false, false, true>, H, gh, gd, params, st); break;
+                case 3: rc = launch_group<BP>(k_batch_backproject<1, false, false, true>, H, gh, gd, params, st); break;
+                case 4: rc = launch_group<BP>(k_batch_backproject<0, false, true, false>, H, gh, gd, params, st); break;
+                case 5: rc = launch_group<BP>(k_batch_backproject<1, false, true, false>, H, gh, gd, params, st); break;
+                case 6: rc = launch_group<BP>(k_batch_backproject<0, false, true, true>, H, gh, gd, params, st); break;
+                case 7: rc = launch_group<BP>(k_batch_backproject<1, false, true, true>, H, gh, gd, params, st); break;
+                case 8: rc = launch_group<BP>(k_batch_backproject<0, true, false, false>, H, gh, gd, params, st); break;
+                case 9: rc = launch_group<BP>(k_batch_backproject<1, true, false, false>, H, gh, gd, params, st); break;
+                default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", H->variant);
+            }
+        }
+        if (rc != APRICT_OK) return rc;
+    }
+    return APRICT_OK;
+}

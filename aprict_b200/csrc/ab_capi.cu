@@ -1,5 +1,6 @@
 // ab_capi.cu -- status strings, version and shared host validation.
 #include <math.h>
+#include <stddef.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -11,6 +12,8 @@ static_assert(sizeof(aprict_vol_desc) == 32, "vol_desc layout");
 static_assert(sizeof(aprict_proj_desc) == 40, "proj_desc layout");
 static_assert(sizeof(aprict_project_config) == 16, "project_config layout");
 static_assert(sizeof(aprict_backproject_config) == 76, "backproject_config layout");
+static_assert(sizeof(aprict_scan) == 120 && offsetof(aprict_scan, vol) == 64 && offsetof(aprict_scan, vol_dev) == 96,
+              "scan layout");
 
 static thread_local char g_last_error[512] = "";
 static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0, 0};
@@ -118,6 +121,7 @@ size_t aprict_b200_struct_size(const char *name) {
     if (!strcmp(name, "aprict_backproject_config")) return sizeof(aprict_backproject_config);
     if (!strcmp(name, "aprict_forbild_shape")) return sizeof(aprict_forbild_shape);
     if (!strcmp(name, "aprict_quadric")) return sizeof(aprict_quadric);
+    if (!strcmp(name, "aprict_scan")) return sizeof(aprict_scan);
     return 0;
 }
 

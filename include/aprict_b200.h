@@ -298,6 +298,50 @@ APRICT_API int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
                                            float multiply_before_adding, uint32_t ssu, uint32_t ssv, int mode,
                                            uint32_t *overflow_dev, uint32_t *status_dev, aprict_stream_t stream);
 
+/* ---- Many scans in one persistent launch ----
+ * No reference counterpart (the reference runs one scan per call). A batch is
+ * a plan built on the host from per-scan arguments -- exactly the arguments
+ * of one aprict_b200_project_siddon / aprict_b200_backproject call each -- and
+ * copied by the caller to device memory; aprict_b200_batch_run then performs
+ * every scan's operation in one launch whose CTAs pull detector tiles (project)
+ * or volume bricks (backproject) of all scans from a counter kept in the plan.
+ * Each scan's result equals that of its one-scan call. */
+enum { APRICT_BATCH_PROJECT = 0, APRICT_BATCH_BACKPROJECT = 1 };
+
+typedef struct {
+    const aprict_proj_spec *specs_dev;
+    aprict_proj_desc projs;
+    float *projs_dev;            /* project: output; backproject: input */
+    const float *base_dev;       /* project only: NULL = accumulate, else fused residual base */
+    aprict_vol_desc vol;
+    float *vol_dev;              /* project: input; backproject: output */
+    const float *multiplier_dev; /* backproject only: iff the scan's config applies one */
+    uint32_t *status_dev;        /* optional */
+} aprict_scan;
+
+/* Bytes a plan of n_scans needs (0 for an invalid op or count). */
+APRICT_API size_t aprict_b200_batch_plan_bytes(int op, int n_scans);
+
+/* Validate the scans (as the one-scan calls would) and write the plan into
+ * plan_host (256-byte aligned, plan_capacity >= plan_bytes). Enqueues no
+ * device work; it queries the current device (multiprocessor count and
+ * occupancy, which also loads the kernels, so a later run inside a stream
+ * capture loads nothing).
+ * configs points to n_scans aprict_project_config (op PROJECT) or
+ * aprict_backproject_config (op BACKPROJECT); a backprojection batch needs
+ * the same volume order and mode (exact / fast / raycast, nearest /
+ * bilinear) in every scan. The plan records the device pointers given here. */
+APRICT_API int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_scans, const void *configs,
+                                      void *plan_host, size_t plan_capacity);
+
+/* Run a plan: plan_dev is a byte copy of plan_host in device memory (256-byte
+ * aligned). The work counters in plan_dev must be zero before the first run
+ * (they are in a fresh copy); each run leaves them zero again, so the same
+ * plan_dev can be run repeatedly or captured in a CUDA graph. Two runs of one
+ * plan_dev must not overlap in time (they would share its counters). A batch
+ * of more than 96 scans runs as one launch per 96 scans. */
+APRICT_API int aprict_b200_batch_run(const void *plan_host, void *plan_dev, aprict_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -146,3 +146,44 @@ def test_tuning_knobs_validate_and_round_trip() -> None:
     finally:
         for k, v in enumerate(saved):
             lib.aprict_b200_set_tuning(k, v)
+
+
+def test_batch_plan_validates_on_the_host() -> None:
+    lib = _lib.lib()
+    assert lib.aprict_b200_batch_plan_bytes(0, 0) == 0
+    assert lib.aprict_b200_batch_plan_bytes(7, 3) == 0
+    n1, n96, n97 = (lib.aprict_b200_batch_plan_bytes(1, k) for k in (1, 96, 97))
+    assert 0 < n1 < n96 < n97
+    assert lib.aprict_b200_batch_plan_bytes(0, 3) > 0
+    raw = np.zeros(n97 + 256, np.uint8)
+    buf = raw[(-raw.ctypes.data) % 256 :]
+    scans = np.zeros(2, S.scan)
+    for i, order in enumerate(("C", "F")):
+        scans[i]["specs_dev"] = _fake()
+        scans[i]["projs"] = _lib.proj_desc((2, 4, 4), (16, 4, 1))
+        scans[i]["projs_dev"] = _fake()
+        scans[i]["vol"] = _lib.vol_desc((4, 4, 4), order, 1.0, np.zeros(3))
+        scans[i]["vol_dev"] = _fake()
+    cfgs = np.zeros(2, S.backproject_config)
+    cfgs["ssx"] = cfgs["ssy"] = cfgs["ssz"] = 1
+    cap = lib.aprict_b200_batch_plan_bytes(1, 2)
+    # unknown op, too small a buffer, misaligned buffer, mixed volume order
+    for op, c, ptr in [(5, cap, buf.ctypes.data), (1, cap - 1, buf.ctypes.data), (1, cap, buf.ctypes.data + 4),
+                       (1, cap, buf.ctypes.data)]:
+        with pytest.raises(ValueError):
+            _lib.check(lib.aprict_b200_batch_plan(op, _lib.ptr(scans), 2, _lib.ptr(cfgs), ptr, c), "batch_plan")
+    assert "same volume order" in lib.aprict_b200_last_error().decode()
+    # a bad scan is reported with its index
+    scans[1]["vol"] = _lib.vol_desc((4, 4, 4), "C", -1.0, np.zeros(3))
+    with pytest.raises(ValueError, match="scan 1"):
+        _lib.check(lib.aprict_b200_batch_plan(1, _lib.ptr(scans), 2, _lib.ptr(cfgs), buf.ctypes.data, cap), "batch_plan")
+    # running something that is not a plan
+    with pytest.raises(ValueError):
+        _lib.check(lib.aprict_b200_batch_run(buf.ctypes.data, buf.ctypes.data, None), "batch_run")
+
+
+def test_batch_records_keep_the_c_layout() -> None:
+    from aprict_b200.batch import _packed
+
+    recs = _packed([np.zeros((), S.scan)] * 3, S.scan)
+    assert recs.dtype.itemsize == _lib.lib().aprict_b200_struct_size(b"aprict_scan") == 120
