@@ -128,11 +128,11 @@ __device__ __forceinline__ void retire(Group *g) {
     }
 }
 
-template <typename Off>
+template <typename Off, bool SS1>
 __global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __grid_constant__ BatchArgs<ab_fp::FPScan<Off>> A) {
     uint32_t unit;
     int s;
-    while (next_unit(A, unit, s)) ab_fp::fp_tile(A.scans[s], unit);
+    while (next_unit(A, unit, s)) ab_fp::fp_tile<Off, SS1>(A.scans[s], unit);
     retire(A.g);
 }
 
@@ -227,7 +227,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
     std::vector<ab_fp::FPScan<int32_t>> fp32(op == APRICT_BATCH_PROJECT ? n_scans : 0);
     std::vector<ab_fp::FPScan<int64_t>> fp64(op == APRICT_BATCH_PROJECT ? n_scans : 0);
     std::vector<ab_bp::BPParams> bp(op == APRICT_BATCH_BACKPROJECT ? n_scans : 0);
-    bool all_small = true;
+    bool all_small = true, all_ss1 = true;
     int variant = -1;
     for (int i = 0; i < n_scans; ++i) {
         const aprict_scan &sc = scans[i];
@@ -237,6 +237,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             rc = ab_fp::fp_check(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, cfg);
             if (rc != APRICT_OK) return scan_error(rc, i);
             all_small = all_small && ab_fp::small_volume(&sc.vol);
+            all_ss1 = all_ss1 && cfg->ssu == 1 && cfg->ssv == 1;
             uint64_t u = 0;
             fp32[i] = ab_fp::make_fpscan<int32_t>(sc.specs_dev, &sc.projs, sc.projs_dev, sc.base_dev, &sc.vol,
                                                   sc.vol_dev, cfg, sc.status_dev, u);
@@ -261,7 +262,8 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             units[i] = u;
         }
     }
-    if (op == APRICT_BATCH_PROJECT) variant = all_small ? 0 : 1;
+    // projection variant: bit 0 = 64-bit offsets, bit 1 = sub-rays (ssu or ssv > 1)
+    if (op == APRICT_BATCH_PROJECT) variant = (all_small ? 0 : 1) | (all_ss1 ? 0 : 2);
 
     // Largest scans first; zero-unit scans are kept (they take no units).
     std::vector<int> order(n_scans);
@@ -294,8 +296,12 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
         int rc = APRICT_OK;
         if (G->n_units > 0) {
             if (op == APRICT_BATCH_PROJECT) {
-                rc = variant == 0 ? grid_for(k_batch_project<int32_t>, G->n_units, G->grid)
-                                  : grid_for(k_batch_project<int64_t>, G->n_units, G->grid);
+                switch (variant) {
+                    case 0: rc = grid_for(k_batch_project<int32_t, true>, G->n_units, G->grid); break;
+                    case 1: rc = grid_for(k_batch_project<int64_t, true>, G->n_units, G->grid); break;
+                    case 2: rc = grid_for(k_batch_project<int32_t, false>, G->n_units, G->grid); break;
+                    default: rc = grid_for(k_batch_project<int64_t, false>, G->n_units, G->grid); break;
+                }
             } else {
                 switch (variant) {
                     case 0: rc = grid_for(k_batch_backproject<0, false, false, false>, G->n_units, G->grid); break;
@@ -318,7 +324,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
     for (int k = 0; k < n_scans; ++k) {
         const int i = order[k];
         if (op == APRICT_BATCH_PROJECT) {
-            if (variant == 0)
+            if ((variant & 1) == 0)
                 memcpy(params + k * sizeof(ab_fp::FPScan<int32_t>), &fp32[i], sizeof(ab_fp::FPScan<int32_t>));
             else
                 memcpy(params + k * sizeof(ab_fp::FPScan<int64_t>), &fp64[i], sizeof(ab_fp::FPScan<int64_t>));
@@ -346,9 +352,15 @@ extern "C" int aprict_b200_batch_run(const void *plan_host, void *plan_dev, apri
         Group *gd = reinterpret_cast<Group *>(db + off);
         int rc;
         if (H->op == APRICT_BATCH_PROJECT) {
-            rc = H->variant == 0
-                     ? launch_group<ab_fp::FPScan<int32_t>>(k_batch_project<int32_t>, H, gh, gd, params, st)
-                     : launch_group<ab_fp::FPScan<int64_t>>(k_batch_project<int64_t>, H, gh, gd, params, st);
+            using F32 = ab_fp::FPScan<int32_t>;
+            using F64 = ab_fp::FPScan<int64_t>;
+            switch (H->variant) {
+                case 0: rc = launch_group<F32>(k_batch_project<int32_t, true>, H, gh, gd, params, st); break;
+                case 1: rc = launch_group<F64>(k_batch_project<int64_t, true>, H, gh, gd, params, st); break;
+                case 2: rc = launch_group<F32>(k_batch_project<int32_t, false>, H, gh, gd, params, st); break;
+                case 3: rc = launch_group<F64>(k_batch_project<int64_t, false>, H, gh, gd, params, st); break;
+                default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", H->variant);
+            }
         } else {
             using BP = ab_bp::BPParams;
             switch (H->variant) {

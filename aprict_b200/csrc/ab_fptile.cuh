@@ -110,36 +110,47 @@ struct FPScan {
 };
 
 // Rays of work unit b (block_tile order) of scan S; every thread of the CTA
-// calls it with the same b. No barriers inside.
-template <typename Off>
+// calls it with the same b. No barriers inside. SS1: one sub-ray per pixel
+// (ssu = ssv = 1), which keeps nothing but the sum live across the traversal.
+template <typename Off, bool SS1>
 __device__ __forceinline__ void fp_tile(const FPScan<Off> &S, uint32_t b) {
     int view, iu, iv;
     block_tile(S.tm, S.n_views, b, view, iu, iv);
     if (iu >= (int)S.nu || iv >= (int)S.nv) return;
-    const aprict_proj_spec sp = S.specs[view];
-    const ab_grid<Off> &g = S.g;
-    const ab_d3 src = ab_to_grid(g, ab_d3_of(sp.source_pos) * (double)S.svf);
-
-    bool bad = false;
-    float tot = 0.f;
     const uint64_t pol = l2_evict_last_policy();
-    const int ssu = S.ssu, ssv = S.ssv;
-    const double inv_su = 1.0 / (double)ssu, inv_sv = 1.0 / (double)ssv;
-    for (int ku = 0; ku < ssu; ++ku) {
-        float accu = 0.f;
-        for (int kv = 0; kv < ssv; ++kv) {
-            const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
-            const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
-            const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)S.svf);
-            VolLoad<Off> ld{S.vol, pol};
-            float sum;
-            ab_siddon_gather<Off>(src, dst, g.n, g.stride, ld, sum, &bad);
-            accu += (sum * g.voxwid) * S.mba;
+    bool bad = false;
+    float tot;
+    if (SS1) {
+        const aprict_proj_spec &sp = S.specs[view];
+        const ab_d3 src = ab_to_grid(S.g, ab_d3_of(sp.source_pos) * (double)S.svf);
+        const ab_d3 dst = ab_to_grid(S.g, ab_pixel_pos(sp, (double)iu, (double)iv) * (double)S.svf);
+        VolLoad<Off> ld{S.vol, pol};
+        float sum;
+        ab_siddon_gather<Off>(src, dst, S.g.n, S.g.stride, ld, sum, &bad);
+        tot = (sum * S.g.voxwid) * S.mba;
+    } else {
+        const aprict_proj_spec sp = S.specs[view];
+        const ab_grid<Off> &g = S.g;
+        const ab_d3 src = ab_to_grid(g, ab_d3_of(sp.source_pos) * (double)S.svf);
+        tot = 0.f;
+        const int ssu = S.ssu, ssv = S.ssv;
+        const double inv_su = 1.0 / (double)ssu, inv_sv = 1.0 / (double)ssv;
+        for (int ku = 0; ku < ssu; ++ku) {
+            float accu = 0.f;
+            for (int kv = 0; kv < ssv; ++kv) {
+                const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
+                const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
+                const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)S.svf);
+                VolLoad<Off> ld{S.vol, pol};
+                float sum;
+                ab_siddon_gather<Off>(src, dst, g.n, g.stride, ld, sum, &bad);
+                accu += (sum * g.voxwid) * S.mba;
+            }
+            if (ssv > 1) accu /= (float)ssv;
+            tot += accu;
         }
-        if (ssv > 1) accu /= (float)ssv;
-        tot += accu;
+        if (ssu > 1) tot /= (float)ssu;
     }
-    if (ssu > 1) tot /= (float)ssu;
     if (bad && S.status) atomicOr(S.status, APRICT_STATUS_NONFINITE);
     const int64_t o = (int64_t)view * S.ps.view + (int64_t)iu * S.ps.u + (int64_t)iv * S.ps.v;
     if (S.base) {

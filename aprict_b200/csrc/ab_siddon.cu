@@ -17,9 +17,12 @@ struct ScatterVisit {
     }
 };
 
-template <typename Off>
+// The one-scan kernel always takes the general sub-ray path: with the scan
+// in the constant bank it measured 2.4 % faster than the single-sub-ray
+// specialisation (which the batch kernel uses, where it removes spills).
+template <typename Off, bool SS1>
 __global__ void __launch_bounds__(kThreads, 4) k_project_siddon(const FPScan<Off> S) {
-    fp_tile(S, blockIdx.x);
+    fp_tile<Off, SS1>(S, blockIdx.x);
 }
 
 template <typename Off>
@@ -66,13 +69,13 @@ extern "C" int aprict_b200_project_siddon(const aprict_proj_spec *specs_dev, con
             make_fpscan<int32_t>(specs_dev, pd, projs_dev, base_dev, vd, vol_dev, cfg, status_dev, nblocks);
         if (nblocks == 0) return APRICT_OK;
         if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
-        k_project_siddon<int32_t><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
+        k_project_siddon<int32_t, false><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
     } else {
         const FPScan<int64_t> S =
             make_fpscan<int64_t>(specs_dev, pd, projs_dev, base_dev, vd, vol_dev, cfg, status_dev, nblocks);
         if (nblocks == 0) return APRICT_OK;
         if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
-        k_project_siddon<int64_t><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
+        k_project_siddon<int64_t, false><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
     }
     return ab_cuda_check(cudaGetLastError(), "project_siddon launch");
 }
