@@ -58,6 +58,7 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
     "aprict_b200_batch_plan_bytes": (ctypes.c_size_t, [_c_int, _c_int]),
     "aprict_b200_batch_plan": (_c_int, [_c_int, _c_void_p, _c_int, _c_void_p, _c_void_p, ctypes.c_size_t]),
     "aprict_b200_batch_run": (_c_int, [_c_void_p, _c_void_p, _c_void_p]),
+    "aprict_b200_batch_run_static": (_c_int, [_c_void_p, _c_void_p]),
     "aprict_b200_project_forbild": (
         _c_int,
         [

@@ -381,3 +381,43 @@ extern "C" int aprict_b200_batch_run(const void *plan_host, void *plan_dev, apri
     }
     return APRICT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batch run without a caller-provided device plan: the work counters live in
+// a fixed static device array instead (no allocation anywhere on this path).
+
+static constexpr size_t kStaticScratchBytes = 8192;  // header slot + 15 launch groups (1440 scans)
+static __device__ __align__(256) unsigned char g_batch_scratch[kStaticScratchBytes];
+static constexpr int kMaxDevices = 64;
+static void *g_scratch_addr[kMaxDevices] = {};
+
+extern "C" int aprict_b200_batch_run_static(const void *plan_host, aprict_stream_t stream) {
+    if (plan_host == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "batch run needs the host plan");
+    const PlanHeader *H = static_cast<const PlanHeader *>(plan_host);
+    if (H->magic != kPlanMagic) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "not a batch plan");
+    // The kernels touch only the Group counters of the device copy, at the
+    // offsets the host image gives them.
+    const size_t need = H->groups_off + (size_t)H->n_groups * align256(sizeof(Group));
+    if (need > kStaticScratchBytes)
+        return ab_fail(APRICT_ERR_TOO_LARGE,
+                       "plan has %d launch groups (%d scans); the static scratch holds at most %zu groups (%zu scans)",
+                       H->n_groups, H->n_scans, (kStaticScratchBytes - H->groups_off) / align256(sizeof(Group)),
+                       (kStaticScratchBytes - H->groups_off) / align256(sizeof(Group)) * (size_t)kGroup);
+    int dev = 0;
+    int rc = ab_cuda_check(cudaGetDevice(&dev), "batch_run_static: cudaGetDevice");
+    if (rc != APRICT_OK) return rc;
+    if (dev < 0 || dev >= kMaxDevices) return ab_fail(APRICT_ERR_TOO_LARGE, "device ordinal %d out of range", dev);
+    void *scratch = __atomic_load_n(&g_scratch_addr[dev], __ATOMIC_ACQUIRE);
+    if (scratch == nullptr) {
+        // First call on this device: look up the array's address (this can
+        // load the module, so make the first call before any stream capture).
+        rc = ab_cuda_check(cudaGetSymbolAddress(&scratch, g_batch_scratch), "batch_run_static: cudaGetSymbolAddress");
+        if (rc != APRICT_OK) return rc;
+        __atomic_store_n(&g_scratch_addr[dev], scratch, __ATOMIC_RELEASE);
+    }
+    // Counters start at zero for every call, whatever an earlier call left.
+    rc = ab_cuda_check(cudaMemsetAsync(scratch, 0, need, reinterpret_cast<cudaStream_t>(stream)),
+                       "batch_run_static: clearing the counters");
+    if (rc != APRICT_OK) return rc;
+    return aprict_b200_batch_run(plan_host, scratch, stream);
+}

@@ -342,6 +342,18 @@ APRICT_API int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
  * of more than 96 scans runs as one launch per 96 scans. */
 APRICT_API int aprict_b200_batch_run(const void *plan_host, void *plan_dev, aprict_stream_t stream);
 
+/* aprict_b200_batch_run for callers that cannot allocate device memory (no
+ * counterpart in the reference). The plan's work counters live in a static
+ * 8 KB device array of the library instead of a caller copy of the plan, so
+ * the caller passes only the host plan: nothing is allocated, copied from
+ * the host, or freed. The counters are cleared (an asynchronous memset on
+ * the stream) at every call. Limits: at most 15 launch groups (1440 scans)
+ * per plan, else APRICT_ERR_TOO_LARGE; the first call on each device looks
+ * the array up (cudaGetSymbolAddress, which may load the module), so make it
+ * before any stream capture; calls that overlap in time on one device share
+ * the array and race, so serialise them (one stream, or events). */
+APRICT_API int aprict_b200_batch_run_static(const void *plan_host, aprict_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
