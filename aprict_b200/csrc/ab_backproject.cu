@@ -40,17 +40,22 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     BPParams P;
     uint64_t grid = 0;
     int xb = 2;
-    const int rc = make_bp_params(specs_dev, pd, projs_dev, vd, vol_dev, multiplier_dev, cfg, status_dev, P, grid, xb);
+    // Slice stacks (one z layer) always take two voxels per thread.
+    const int rc = make_bp_params(specs_dev, pd, projs_dev, vd, vol_dev, multiplier_dev, cfg, status_dev, P, grid, xb,
+                                  vd != nullptr && bp_ord(vd) == 2 ? 2 : 0);
     if (rc != APRICT_OK || grid == 0) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const bool lin = cfg->approx_mode_linear_interpolate != 0;
-    if (xb == 4) {
-        if (vd->order == 0)
+    const int ord = bp_ord(vd);
+    if (ord == 2) {
+        launch_bp<2, 2>(P, cfg, lin, (unsigned)grid, st);  // slices (xb forced to 2 below)
+    } else if (xb == 4) {
+        if (ord == 0)
             launch_bp<0, 4>(P, cfg, lin, (unsigned)grid, st);
         else
             launch_bp<1, 4>(P, cfg, lin, (unsigned)grid, st);
     } else {
-        if (vd->order == 0)
+        if (ord == 0)
             launch_bp<0, 2>(P, cfg, lin, (unsigned)grid, st);
         else
             launch_bp<1, 2>(P, cfg, lin, (unsigned)grid, st);

@@ -145,12 +145,42 @@ __global__ void __launch_bounds__(ab_bp::kThreads, 3) k_batch_backproject(const 
     retire(A.g);
 }
 
-// Backprojection kernel variant code: ORD | mode << 1, mode 0 fast nearest,
-// 1 fast bilinear, 2 raycast nearest, 3 raycast bilinear, 4 exact.
-int bp_variant(const aprict_backproject_config *c, uint32_t order) {
+// Backprojection kernel variant code: ORD + 3 * mode (ORD from ab_bp::bp_ord),
+// mode 0 fast nearest, 1 fast bilinear, 2 raycast nearest, 3 raycast
+// bilinear, 4 exact.
+int bp_variant(const aprict_backproject_config *c, const aprict_vol_desc *vd) {
     const int mode = c->exact ? 4
                               : (c->approx_mode_direct_raycast ? 2 : 0) + (c->approx_mode_linear_interpolate ? 1 : 0);
-    return (int)order | (mode << 1);
+    return ab_bp::bp_ord(vd) + 3 * mode;
+}
+
+// The batch backprojection kernel of a variant code.
+template <int V>
+auto bp_kernel() {
+    constexpr int ORD = V % 3, mode = V / 3;
+    return k_batch_backproject<ORD, mode == 4, mode == 2 || mode == 3, mode == 1 || mode == 3>;
+}
+
+template <class F>
+int with_bp_kernel(int variant, F &&f) {
+    switch (variant) {
+        case 0: return f(bp_kernel<0>());
+        case 1: return f(bp_kernel<1>());
+        case 2: return f(bp_kernel<2>());
+        case 3: return f(bp_kernel<3>());
+        case 4: return f(bp_kernel<4>());
+        case 5: return f(bp_kernel<5>());
+        case 6: return f(bp_kernel<6>());
+        case 7: return f(bp_kernel<7>());
+        case 8: return f(bp_kernel<8>());
+        case 9: return f(bp_kernel<9>());
+        case 10: return f(bp_kernel<10>());
+        case 11: return f(bp_kernel<11>());
+        case 12: return f(bp_kernel<12>());
+        case 13: return f(bp_kernel<13>());
+        case 14: return f(bp_kernel<14>());
+        default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", variant);
+    }
 }
 
 int sm_count(int &sms) {
@@ -252,11 +282,12 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
                                        cfg, sc.status_dev, bp[i], u, xb, 2);
             if (rc != APRICT_OK) return scan_error(rc, i);
-            const int v = bp_variant(cfg, sc.vol.order);
+            const int v = bp_variant(cfg, &sc.vol);
             if (variant >= 0 && v != variant)
                 return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
-                               "scan %d: every scan of a backprojection batch needs the same volume order and "
-                               "backprojection mode (exact / fast / raycast, nearest / bilinear)",
+                               "scan %d: every scan of a backprojection batch needs the same volume order, "
+                               "slice form (one z layer or more) and backprojection mode (exact / fast / raycast, "
+                               "nearest / bilinear)",
                                i);
             variant = v;
             units[i] = u;
@@ -303,19 +334,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
                     default: rc = grid_for(k_batch_project<int64_t, false>, G->n_units, G->grid); break;
                 }
             } else {
-                switch (variant) {
-                    case 0: rc = grid_for(k_batch_backproject<0, false, false, false>, G->n_units, G->grid); break;
-                    case 1: rc = grid_for(k_batch_backproject<1, false, false, false>, G->n_units, G->grid); break;
-                    case 2: rc = grid_for(k_batch_backproject<0, false, false, true>, G->n_units, G->grid); break;
-                    case 3: rc = grid_for(k_batch_backproject<1, false, false, true>, G->n_units, G->grid); break;
-                    case 4: rc = grid_for(k_batch_backproject<0, false, true, false>, G->n_units, G->grid); break;
-                    case 5: rc = grid_for(k_batch_backproject<1, false, true, false>, G->n_units, G->grid); break;
-                    case 6: rc = grid_for(k_batch_backproject<0, false, true, true>, G->n_units, G->grid); break;
-                    case 7: rc = grid_for(k_batch_backproject<1, false, true, true>, G->n_units, G->grid); break;
-                    case 8: rc = grid_for(k_batch_backproject<0, true, false, false>, G->n_units, G->grid); break;
-                    case 9: rc = grid_for(k_batch_backproject<1, true, false, false>, G->n_units, G->grid); break;
-                    default: rc = ab_fail(APRICT_ERR_INVALID_ARGUMENT, "unsupported backprojection mode");
-                }
+                rc = with_bp_kernel(variant, [&](auto k) { return grid_for(k, G->n_units, G->grid); });
             }
         }
         if (rc != APRICT_OK) return rc;
@@ -362,20 +381,9 @@ extern "C" int aprict_b200_batch_run(const void *plan_host, void *plan_dev, apri
                 default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", H->variant);
             }
         } else {
-            using BP = ab_bp::BPParams;
-            switch (H->variant) {
-                case 0: rc = launch_group<BP>(k_batch_backproject<0, false, false, false>, H, gh, gd, params, st); break;
-                case 1: rc = launch_group<BP>(k_batch_backproject<1, false, false, false>, H, gh, gd, params, st); break;
-                case 2: rc = launch_group<BP>(k_batch_backproject<0, false, false, true>, H, gh, gd, params, st); break;
-                case 3: rc = launch_group<BP>(k_batch_backproject<1, false, false, true>, H, gh, gd, params, st); break;
-                case 4: rc = launch_group<BP>(k_batch_backproject<0, false, true, false>, H, gh, gd, params, st); break;
-                case 5: rc = launch_group<BP>(k_batch_backproject<1, false, true, false>, H, gh, gd, params, st); break;
-                case 6: rc = launch_group<BP>(k_batch_backproject<0, false, true, true>, H, gh, gd, params, st); break;
-                case 7: rc = launch_group<BP>(k_batch_backproject<1, false, true, true>, H, gh, gd, params, st); break;
-                case 8: rc = launch_group<BP>(k_batch_backproject<0, true, false, false>, H, gh, gd, params, st); break;
-                case 9: rc = launch_group<BP>(k_batch_backproject<1, true, false, false>, H, gh, gd, params, st); break;
-                default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", H->variant);
-            }
+            rc = with_bp_kernel(H->variant, [&](auto k) {
+                return launch_group<ab_bp::BPParams>(k, H, gh, gd, params, st);
+            });
         }
         if (rc != APRICT_OK) return rc;
     }

@@ -59,6 +59,7 @@ struct BPParams {
     float sep, inv_sep;
     int pL, pV;
     float val;
+    float inv_val;  // 1 / val
     int ssx, ssy, ssz;
     uint32_t *status;
 };
@@ -137,10 +138,21 @@ __device__ __forceinline__ float taper(const ab_bpview &b, float fu, float fv, f
     return ab_edge_taper(fu - b.cu0, fv - b.cv0, b.inv_halfu, b.inv_halfv, inv_sep);
 }
 
+// x^e for a small integer e with one approximate reciprocal for e < 0
+// (relative error ~1e-6; the reference divides e times, CB_backproject.cu:21-35).
+__device__ __forceinline__ float powi_fast(float x, int e) {
+    const float r = e < 0 ? rcp_fast(x) : x;
+    const int n = e < 0 ? -e : e;
+    float a = 1.f;
+    for (int k = 0; k < n; ++k) a *= r;
+    return a;
+}
+
+// (Z/L)^pL (Z/val)^pV, the direct-raycast weights (CB_backproject.cu:512-528).
 __device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, float Z) {
     float w = 1.f;
-    if (P.pL != 0) w *= ab_powint(Z * b.invL, P.pL);
-    if (P.pV != 0) w *= ab_powint(Z / P.val, P.pV);
+    if (P.pL != 0) w *= powi_fast(Z * b.invL, P.pL);
+    if (P.pV != 0) w *= powi_fast(Z * P.inv_val, P.pV);
     return w;
 }
 
@@ -181,10 +193,16 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     if (b1 >= P.gb[1] || b2 >= P.gb[2]) return;  // the whole CTA returns before any barrier
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Axes: a0 along the lanes (memory-contiguous), a1 along the warps, a2
+    // along each thread's XB voxels. ORD 0: C order (z, y, x); ORD 1: F order
+    // (x, y, z); ORD 2: C order with nz == 1 (slices): lanes along y (stride
+    // 1), warps and XB both along x, z = 0.
+    constexpr int a0 = ORD == 0 ? 2 : (ORD == 1 ? 0 : 1);
+    constexpr int a1 = ORD == 2 ? 2 : 1;
+    constexpr int a2 = ORD == 1 ? 2 : 0;
     const int i0 = b0 * 32 + lane;
-    const int i1 = b1 * 8 + warp;
-    const int i2b = b2 * kXB;
-    constexpr int a0 = ORD == 0 ? 2 : 0, a1 = 1, a2 = ORD == 0 ? 0 : 2;
+    const int i1 = ORD == 2 ? 0 : b1 * 8 + warp;
+    const int i2b = ORD == 2 ? (b1 * 8 + warp) * kXB : b2 * kXB;
     const bool in01 = i0 < P.n[a0] && i1 < P.n[a1];
 
     // Voxel-centre coordinates relative to the volume centre, per axis.
@@ -446,6 +464,11 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     }
 }
 
+// Host: the kernel's axis assignment for a volume (see bp_brick): 0 C order,
+// 1 F order, 2 C order with one z layer (slice stacks of fan-beam scans),
+// where lanes run along y instead of the single z layer.
+inline int bp_ord(const aprict_vol_desc *vd) { return vd->order == 0 ? (vd->nz == 1 && vd->ny > 1 ? 2 : 0) : 1; }
+
 // Host: validate one backprojection call and fill its parameters; units is
 // the number of work units (bricks, 0 when empty), xb the voxels per thread
 // (force_xb 2 or 4, or 0 for the tuning knob's choice).
@@ -519,6 +542,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.pL = cfg->Z_on_L_factor_power;
     P.pV = cfg->Z_on_val_factor_power;
     P.val = cfg->Z_on_val_factor_val;
+    P.inv_val = P.val != 0.f ? (float)(1.0 / (double)P.val) : 0.f;
     P.ssx = (int)cfg->ssx;
     P.ssy = (int)cfg->ssy;
     P.ssz = (int)cfg->ssz;
@@ -526,10 +550,17 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
 
     xb = force_xb == 2 || force_xb == 4 ? force_xb : (ab_tuning_get(AB_TUNE_BP_XB) == 4 ? 4 : 2);
     const int kXB = xb;
-    const int n0 = vd->order == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = vd->order == 0 ? P.n[0] : P.n[2];
-    P.gb[0] = (n0 + 31) / 32;
-    P.gb[1] = (n1 + 7) / 8;
-    P.gb[2] = (n2 + kXB - 1) / kXB;
+    const int ord = bp_ord(vd);
+    if (ord == 2) {  // slices: lanes along y, warps x XB along x
+        P.gb[0] = (P.n[1] + 31) / 32;
+        P.gb[1] = (P.n[0] + 8 * kXB - 1) / (8 * kXB);
+        P.gb[2] = 1;
+    } else {
+        const int n0 = ord == 0 ? P.n[2] : P.n[0], n1 = P.n[1], n2 = ord == 0 ? P.n[0] : P.n[2];
+        P.gb[0] = (n0 + 31) / 32;
+        P.gb[1] = (n1 + 7) / 8;
+        P.gb[2] = (n2 + kXB - 1) / kXB;
+    }
     // Super-brick: all blocks of the fastest axis x sb1 x sb2 blocks (8 and
     // kXB voxels each), about one wave of resident CTAs, with equal extents in
     // voxels along the middle and slowest axes.

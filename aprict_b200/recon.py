@@ -80,3 +80,46 @@ def fbp_fan_circ(
     )
     fp.backproject(cfg, volume, fp.ProjectionSet(projs.proj_geom, data=filtered))
     return volume
+
+
+def fbp_fan_circ_batch(
+    projs: list[fp.ProjectionSet],
+    volumes: list[Volume],
+    *,
+    apodization: str | None = None,
+    interpolate: bool = False,
+    stacked: torch.Tensor | None = None,
+) -> list[Volume]:
+    """Fan-beam FBP of many slices (each a scan with nv = 1) in two launches.
+
+    Every slice must share the fan geometry (R, L, pixel pitch, nu) and view
+    count, as the slices of one fan-beam stack do; then one ramp-filter launch
+    filters all sinograms (``stacked``: an (S*M, nu, 1) tensor holding them,
+    filtered in place into a new buffer; assembled from ``projs`` if None) and
+    one persistent backprojection launch (:class:`~aprict_b200.batch.ScanBatch`)
+    backprojects every slice into its volume. Each slice's result equals
+    :func:`fbp_fan_circ` on that slice.
+    """
+    from .batch import ScanBatch  # noqa: PLC0415
+
+    if not projs or len(projs) != len(volumes):
+        msg = "one volume per sinogram, at least one"
+        raise ValueError(msg)
+    geo = [fan_geometry(p.proj_geom) for p in projs]
+    m = projs[0].proj_geom.num_projs
+    if any(not np.allclose(g, geo[0]) for g in geo) or any(p.proj_geom.num_projs != m for p in projs):
+        msg = "batched fan FBP needs one fan geometry and view count for every slice"
+        raise NotImplementedError(msg)
+    R, L, pixwid, nu, nv = geo[0]  # noqa: N806
+    if stacked is None:
+        stacked = torch.cat([p.data for p in projs], dim=0)
+    filt = FBPFilterer(L=L, physpixwid=pixwid, proj_2d_shape=(nu, nv), _hacky_fan_beam_mode=True, apodization=apodization)
+    (filtered,) = filt.rfilt.filter(stacked, weights=filt._weights, scale=1.0 / (4.0 * np.pi * R * m))  # noqa: SLF001
+    support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
+    cfg = fp.ConfigBackproject(
+        fast_approx=True, cyl_mask_rad=support, Z_on_val_factor_power=-2, Z_on_val_factor_val=R,
+        approx_mode_direct_raycast=True, approx_mode_bilinear_interpolate=interpolate,
+    )
+    views = [fp.ProjectionSet(p.proj_geom, data=filtered[i * m : (i + 1) * m]) for i, p in enumerate(projs)]
+    ScanBatch(volumes, views).backproject(cfg)
+    return volumes

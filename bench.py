@@ -47,6 +47,15 @@ WORKLOADS = {
     "small": dict(n=96, voxwid=1.0, n_ellipsoids=10, views=90, det=128, pix_at_iso=0.8, R=300.0, LmR=300.0, photons=1e5, seed=1),
     # 48 uneven scans: edge log-U(64, 320), views U(90, 720), detector U(128, 768)^2,
     # circular or helical (pitch U(0.5, 1.5)), +-2 mm / +-0.5 deg per-view jitter.
+    # Component workloads (each prints its own line):
+    # fpbp128 -- 128^3 x 1 mm, 10 ellipsoids, 180 views on 256^2 x 1 mm, SOD 500, SDD 1000;
+    # fbp64 -- 64 fan-beam slices 512^2 x 0.5 mm, 720 views, 1024 x 0.4 mm, SOD 600, SDD 1100;
+    # quadric -- 100 clipped quadrics (60 ellipsoids, 40 elliptic cylinders) in 200 mm,
+    #   720 views on 1024^2 x 0.3 mm, SOD 700, SDD 1200, additive densities.
+    "fpbp128": dict(n=128, voxwid=1.0, n_ellipsoids=10, views=180, det=256, pix_at_iso=0.5, R=500.0, LmR=500.0, seed=3),
+    "fbp64": dict(slices=64, n=512, voxwid=0.5, n_ellipses=20, views=720, det=1024, pix=0.4, R=600.0, LmR=500.0, seed=7),
+    "quadric": dict(n_ellipsoids=60, n_cylinders=40, radius=100.0, views=720, det=1024, pix=0.3, R=700.0, LmR=500.0,
+                    seed=11),
     "batch48": dict(n_scans=48, edge=(64, 320), views=(90, 720), det=(128, 768), voxwid=0.5, n_ellipsoids=10,
                     R=500.0, LmR=500.0, photons=1e5, seed=5),
 }
@@ -408,7 +417,7 @@ def run_reference(args) -> dict:
     rank, world, _ = _env_rank()
     if rank != 0:
         return {}
-    if args.workload == "batch48":
+    if args.workload not in ("sirt256", "small"):
         return {"impl": "reference", "unavailable": "the CPU reference arm is timed on the sirt256 workload only"}
     w = WORKLOADS[args.workload]
     pg, x_true = make_problem(w)
@@ -614,6 +623,134 @@ def run_batch(args) -> dict:
     return out if rank == 0 else {}
 
 
+def _timed(fn, k: int) -> float:
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(k):
+        fn()
+    e.record()
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / k
+
+
+def _line(args, metric: str, value: float, unit: str, ms: float, workload: str, extra: dict) -> dict:
+    out = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded phantoms)", "config": {"workload": workload, "baseline_metric": BASELINE_METRIC},
+    }
+    out.update(extra)
+    return out
+
+
+def run_component(args) -> dict:
+    """The fpbp128, fbp64 and quadric workloads (component measurements)."""
+    import torch
+
+    from aprict_b200 import FBVolume, Volume, phantoms
+    from aprict_b200.cb import flatpanel as fp
+    from aprict_b200.recon import fbp_fan_circ, fbp_fan_circ_batch
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    peak, peak_kind = load_peaks()
+    if args.workload == "fpbp128":
+        n = w["n"]
+        pg = fp.ProjGeom.new_circular_scan(num_source_points=w["views"], R=w["R"], L_minus_R=w["LmR"],
+                                           pix_widhei_at_isocenter=(w["pix_at_iso"],) * 2, num_pix_widhei=(w["det"],) * 2)
+        x = Volume(phantoms.ellipsoid_volume(w["seed"], w["n_ellipsoids"], (n, n, n), w["voxwid"], semi_axes_vox=(5, 40)),
+                   voxwid=w["voxwid"])
+        ps = fp.ProjectionSet(pg, data=None)
+        ps.create_buffer()
+        y = fp.ProjectionSet(pg, data=torch.rand_like(ps.data))
+        rays, vv = w["views"] * w["det"] ** 2, n**3 * w["views"]
+        t_fp = _timed(lambda: fp.project(fp.ConfigProject(), x, ps), args.steps)
+        out_v = Volume.zeros((n, n, n), voxwid=w["voxwid"])
+        t_ex = _timed(lambda: fp.backproject(fp.ConfigBackproject(), out_v, y), args.steps)
+        t_near = _timed(lambda: fp.backproject(fp.ConfigBackproject(fast_approx=True), out_v, y), args.steps)
+        t_lin = _timed(lambda: fp.backproject(fp.ConfigBackproject(fast_approx=True, approx_mode_bilinear_interpolate=True),
+                                              out_v, y), args.steps)
+        t_adj = _timed(lambda: fp.backproject_adjoint(fp.ConfigProject(), out_v, y), args.steps)
+        nseg, _ = count_segments(pg, (n, n, n), w["voxwid"])
+        fp_gbs = (4.0 * nseg + 4.0 * rays) / (t_fp * 1e-3) / 1e9
+        extra = {
+            "components": {
+                "fp_ms": round(t_fp, 4), "bp_exact_ms": round(t_ex, 4), "bp_fast_nearest_ms": round(t_near, 4),
+                "bp_fast_bilinear_ms": round(t_lin, 4), "adjoint_scatter_ms": round(t_adj, 4),
+                "fwd_rays_per_s": round(rays / (t_fp * 1e-3), 1),
+                "back_exact_voxel_updates_per_s": round(vv / (t_ex * 1e-3), 1),
+                "back_fast_voxel_updates_per_s": round(vv / (t_near * 1e-3), 1),
+            },
+            "roofline": {"bound": "hbm", "kernel": "project_siddon", "achieved": round(fp_gbs, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(fp_gbs / peak, 4), "traffic": None, "peak_kind": peak_kind},
+        }
+        if not args.no_cpu_baseline:
+            from oracle import oracle
+
+            sel = np.linspace(0, w["views"], 6, endpoint=False).astype(int)
+            corner = -np.float32(w["voxwid"]) * np.array((n, n, n), np.float32) / 2
+            t0 = time.perf_counter()
+            (oracle.ref_project_siddon if oracle.have_ref() else oracle.project_siddon)(
+                pg.to_proj_spec_array()[sel], x.as_numpy(), voxwid=w["voxwid"], corner=corner)
+            dt = time.perf_counter() - t0
+            extra["cpu_baseline"] = {"value": round(len(sel) * w["det"] ** 2 / dt, 1), "unit": "rays/s",
+                                     "cores": os.cpu_count() or 1, "kind": "reference" if oracle.have_ref() else "port",
+                                     "sample": f"forward projection of {len(sel)} of {w['views']} views"}
+        return _line(args, "fwd rays/s", round(rays / (t_fp * 1e-3), 1), "rays/s", t_fp,
+                     f"fpbp128: {n}^3 x {w['voxwid']} mm, {w['views']} views x {w['det']}^2", extra)
+    if args.workload == "fbp64":
+        n, S, m, nu = w["n"], w["slices"], w["views"], w["det"]
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pg = fp.ProjGeom.new_circular_scan(num_source_points=m, R=w["R"], L_minus_R=w["LmR"],
+                                           pix_widhei_at_isocenter=(w["pix"] * w["R"] / L,) * 2, num_pix_widhei=(nu, 1))
+        projs = []
+        for k in range(S):
+            xs = phantoms.ellipsoid_volume(w["seed"] * 100 + k, w["n_ellipses"], (n, n, 1), w["voxwid"],
+                                           semi_axes_vox=(8, 160), rho=(0.05, 1.0))
+            ps = fp.ProjectionSet(pg, data=None)
+            fp.project(fp.ConfigProject(), Volume(xs, voxwid=w["voxwid"]), ps)
+            projs.append(ps)
+        stacked = torch.cat([p.data for p in projs], dim=0)
+        vols = [Volume.zeros((n, n, 1), voxwid=w["voxwid"]) for _ in range(S)]
+        t_b = _timed(lambda: fbp_fan_circ_batch(projs, vols, apodization="hann", stacked=stacked), args.steps)
+
+        def per_slice() -> None:
+            for p, v in zip(projs, vols):
+                fbp_fan_circ(p, v, apodization="hann")
+
+        t_s = _timed(per_slice, max(1, args.steps // 2))
+        vv = S * n * n * m
+        extra = {"components": {"batched_ms": round(t_b, 3), "per_slice_ms": round(t_s, 3),
+                                "batched_over_per_slice": round(t_s / t_b, 3),
+                                "back_voxel_updates_per_s": round(vv / (t_b * 1e-3), 1),
+                                "filtered_samples_per_s": round(S * m * nu / (t_b * 1e-3), 1)}}
+        return _line(args, "fan FBP slices/s", round(S / (t_b * 1e-3), 2), "slices/s", t_b,
+                     f"fbp64: {S} slices {n}^2 x {w['voxwid']} mm, {m} views x {nu} x {w['pix']} mm, Ram-Lak + Hann", extra)
+    # quadric
+    shapes = phantoms.random_quadric_phantom(w["seed"], n_ellipsoids=w["n_ellipsoids"], n_cylinders=w["n_cylinders"],
+                                             radius=w["radius"])
+    L = w["R"] + w["LmR"]  # noqa: N806
+    pg = fp.ProjGeom.new_circular_scan(num_source_points=w["views"], R=w["R"], L_minus_R=w["LmR"],
+                                       pix_widhei_at_isocenter=(w["pix"] * w["R"] / L,) * 2, num_pix_widhei=(w["det"],) * 2)
+    ps = fp.ProjectionSet(pg, data=None)
+    ps.create_buffer()
+    vol = FBVolume(shapes)
+    cfg = fp.ConfigProject(overlap_addition=True)
+    t_q = _timed(lambda: fp.project(cfg, vol, ps), args.steps)
+    rays = w["views"] * w["det"] ** 2
+    extra = {"components": {"project_ms": round(t_q, 3), "rays_per_s": round(rays / (t_q * 1e-3), 1),
+                            "overflow_rays": int(ps.out_of_mem_count),
+                            "output_GB": round(4 * rays / 1e9, 3),
+                            "output_write_GBps": round(4 * rays / (t_q * 1e-3) / 1e9, 1)}}
+    return _line(args, "quadric projection rays/s", round(rays / (t_q * 1e-3), 1), "rays/s", t_q,
+                 f"quadric: {len(shapes)} clipped quadrics in {2 * w['radius']:.0f} mm, {w['views']} views x {w['det']}^2 x {w['pix']} mm, additive", extra)
+
+
 def profile_kernels(args) -> dict:
     """Launch the workload's kernels a few times and exit (a small driver for ncu captures).
 
@@ -622,10 +759,35 @@ def profile_kernels(args) -> dict:
     """
     import torch
 
-    from aprict_b200 import Volume
+    from aprict_b200 import FBVolume, Volume, phantoms
     from aprict_b200.cb import flatpanel as fp
 
     w = WORKLOADS[args.workload]
+    if args.workload == "quadric":  # 4 views of the quadric workload: one analytic-projector launch per step
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pg = fp.ProjGeom.new_circular_scan(num_source_points=4, R=w["R"], L_minus_R=w["LmR"],
+                                           pix_widhei_at_isocenter=(w["pix"] * w["R"] / L,) * 2,
+                                           num_pix_widhei=(w["det"],) * 2)
+        ps = fp.ProjectionSet(pg, data=None)
+        vol = FBVolume(phantoms.random_quadric_phantom(w["seed"], n_ellipsoids=w["n_ellipsoids"],
+                                                       n_cylinders=w["n_cylinders"], radius=w["radius"]))
+        for _ in range(args.steps):
+            fp.project(fp.ConfigProject(overlap_addition=True), vol, ps)
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": args.steps}
+    if args.workload == "fbp64":  # 8 slices: one ramp-filter launch and one batched backprojection per step
+        from aprict_b200.recon import fbp_fan_circ_batch
+
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pg = fp.ProjGeom.new_circular_scan(num_source_points=w["views"], R=w["R"], L_minus_R=w["LmR"],
+                                           pix_widhei_at_isocenter=(w["pix"] * w["R"] / L,) * 2,
+                                           num_pix_widhei=(w["det"], 1))
+        projs = [fp.ProjectionSet(pg, data=torch.rand((w["views"], w["det"], 1), device="cuda")) for _ in range(8)]
+        vols = [Volume.zeros((w["n"], w["n"], 1), voxwid=w["voxwid"]) for _ in range(8)]
+        for _ in range(args.steps):
+            fbp_fan_circ_batch(projs, vols, apodization="hann")
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": 2 * args.steps}
     n = w["n"]
     pg, x_true = make_problem(w)
     b = simulate_data(pg, x_true, w)
@@ -662,6 +824,8 @@ def main() -> None:
             out = run_reference(args)
         elif args.workload == "batch48":
             out = run_batch(args)
+        elif args.workload in ("fpbp128", "fbp64", "quadric"):
+            out = run_component(args)
         else:
             out = run_ours(args)
     if out:

@@ -163,3 +163,18 @@ def test_exact_backprojection_is_adjoint_of_projection() -> None:
     lhs = float((ax.data.double().cpu() * torch.from_numpy(projs).double()).sum())
     rhs = float((vol.astype(np.float64) * aty.astype(np.float64)).sum())
     assert abs(lhs - rhs) / abs(lhs) <= 1e-6
+
+
+@pytest.mark.parametrize("case", ["exact", "fast-nearest", "fast-bilinear", "fast-taper-mask", "raycast-fbp"])
+def test_single_slice_volumes(case: str) -> None:
+    """Volumes with one z layer (fan-beam slice stacks) use a lane-along-y mapping."""
+    shape = (70, 45, 1)
+    cfg = fp.ConfigBackproject(**CASES[case])
+    pg = circular(16, 120, 120, 0.537, 96, 4)
+    projs = _projs(pg, 6)
+    v = Volume.zeros(shape, voxwid=1.0, pos_c=(0.7, -0.4, 0.3))
+    fp.backproject(cfg, v, fp.ProjectionSet(pg, data=torch.from_numpy(projs).cuda()), block=True)
+    corner = np.array((0.7, -0.4, 0.3), np.float32) - np.array(shape, np.float32) / 2
+    want = O.backproject(pg.to_proj_spec_array(), projs, shape, cfg.contents, voxwid=1.0, corner=corner)
+    assert np.linalg.norm(want) > 0
+    assert rel_l2(v.as_numpy(), want) <= TOL

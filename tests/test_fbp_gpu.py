@@ -69,3 +69,24 @@ def test_fbp_reconstructs_phantom() -> None:
     err = np.linalg.norm((rec - x)[inside]) / np.linalg.norm(x[inside])
     assert err < 0.35, err  # discretised FBP of a piecewise-constant phantom: edges dominate the error
     assert abs(rec[inside].mean() - x[inside].mean()) < 0.05 * x[inside].mean()
+
+
+def test_batched_slices_equal_single_slice_fbp() -> None:
+    from aprict_b200.recon import fbp_fan_circ_batch
+
+    n = 64
+    pgs = circular(120, 120.0, 100.0, 0.5123, 128, 1, theta0=0.0)
+    projs, singles = [], []
+    for k in range(5):
+        x = phantoms.ellipsoid_volume(40 + k, 6, (n, n, 1), 0.5, semi_axes_vox=(3, 20))
+        ps = fp.ProjectionSet(pgs, data=None)
+        fp.project(fp.ConfigProject(), Volume(x, voxwid=0.5), ps, block=True)
+        projs.append(ps)
+        one = Volume.zeros((n, n, 1), voxwid=0.5)
+        fbp_fan_circ(ps, one, apodization="hann")
+        singles.append(one.as_numpy())
+    outs = [Volume.zeros((n, n, 1), voxwid=0.5) for _ in range(5)]
+    fbp_fan_circ_batch(projs, outs, apodization="hann")
+    for o, w in zip(outs, singles):
+        assert np.linalg.norm(w) > 0
+        assert rel_l2(o.as_numpy(), w) <= 1e-6
