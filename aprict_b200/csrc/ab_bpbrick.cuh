@@ -38,7 +38,6 @@ struct BPParams {
     int64_t stride_view;
     int su, sv;  // u, v element strides (in-view offsets are checked to fit 32 bits)
     float fnu1, fnv1;  // nu + 1, nv + 1: clamp bounds for the rounded pixel index
-    float tie;         // |f - round(f)| above this is settled in FP64
     const float *projs;
     float *vol;
     const float *mult;
@@ -65,12 +64,11 @@ struct BPParams {
 };
 
 // Pixel index with the reference's zero-order rule (get_zero_interp,
-// CB_backproject.cu:256-271): floor(f + 0.5). The FP32 estimate of f has an
-// error of ~1.1e-4 pixel on a 384-pixel detector plus ~1 ulp of f from the
-// approximate reciprocal (emulated over a 360-view circular scan), growing
-// with the detector size. When f lies within refine = 2e-3 * max(1, n/1024)
-// of a half-integer the choice is made again in FP64 from the voxel's exact
-// position; the kernel receives tie = 1/2 - refine.
+// CB_backproject.cu:256-271): floor(f + 0.5). The FP32 estimate of f carries
+// an error below a per-view a priori bound (ab_fp32_pixel_error_bound; about
+// 5e-4 pixel on a 384-pixel detector, 1e-4 observed). When f lies within 1.5x
+// that bound of a half-integer (|f - round(f)| > tie_u / tie_v of the view)
+// the choice is made again in FP64 from the voxel's exact position.
 
 // x + 1.5 * 2^23 rounds x to the nearest integer (ties to even), which then
 // sits in the low mantissa bits; valid for |x| < 2^22 (the clamp ensures it,
@@ -258,7 +256,10 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
                                         P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
                         const aprict_proj_spec sp = P.specs[v0 + t];
-                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, sv[t], kNear ? &svd[t] : nullptr) && P.status)
+                        // every projected point lies within n/2 + 1 voxels of the centre
+                        const double hext[3] = {(0.5 * P.n[0] + 1.0) * P.vwd, (0.5 * P.n[1] + 1.0) * P.vwd,
+                                                (0.5 * P.n[2] + 1.0) * P.vwd};
+                        if (!ab_derive_bpview(sp, c0d, vw, P.sep, hext, sv[t], kNear ? &svd[t] : nullptr) && P.status)
                             atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
                     }
@@ -395,7 +396,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                     const float tu = __fadd_rn(fu, kMagic), tv = __fadd_rn(fv, kMagic);
                                     const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
                                     const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
-                                    fast = inner && fabsf(du) <= P.tie && fabsf(dv) <= P.tie;
+                                    fast = inner && fabsf(du) <= b.tie_u && fabsf(dv) <= b.tie_v;
                                     // pixel offset from the rounded indices (bits - magic)
                                     const int off = (__float_as_int(tu) - 0x4B400000) * P.su + (__float_as_int(tv) - 0x4B400000) * P.sv;
                                     if (live[k] && fast) pv = __ldg(pvw + off);
@@ -421,7 +422,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                         float du, dv;
                                         int iu = round_index(fu, -2.f, P.fnu1, du);
                                         int iv = round_index(fv, -2.f, P.fnv1, dv);
-                                        const bool tu = fabsf(du) > P.tie, tv = fabsf(dv) > P.tie;
+                                        const bool tu = fabsf(du) > b.tie_u, tv = fabsf(dv) > b.tie_v;
                                         if (tu || tv) {
                                             int id[3];
                                             id[a0] = i0;
@@ -510,7 +511,6 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.sv = (int)pd->stride_v;
     P.fnu1 = (float)pd->nu + 1.f;
     P.fnv1 = (float)pd->nv + 1.f;
-    P.tie = 0.5f - 2e-3f * fmaxf(1.f, (float)(pd->nu > pd->nv ? pd->nu : pd->nv) / 1024.f);
     P.projs = projs_dev;
     P.vol = vol_dev;
     P.mult = multiplier_dev;
