@@ -161,12 +161,19 @@ __device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, flo
 // XB: voxels per thread along the slowest axis (4: more reuse of each view's
 // coefficients, 2: fewer registers and more resident warps).
 // Shared-memory staging of one chunk of per-view coefficients.
+// Fast modes also keep, per warp, a queue of deferred voxel-views (see
+// bp_brick) and the per-(lane, voxel) sums of their contributions.
+constexpr int kWarps = kThreads / 32;
+constexpr int kQCap = 32 + 32 * 4;  // a flush leaves < 32; one view adds <= 32 * XB
+
 template <bool EXACT, bool BILIN>
 struct BPSmem {
     static constexpr bool kNear = !EXACT && !BILIN;
     ab_bpview sv[kChunk];
     ab_bpview_d svd[kNear ? kChunk : 1];
     ab_bpview_exact sx[EXACT ? kChunk : 1];
+    uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];   // (view in chunk) << 7 | k << 5 | lane
+    float qd[EXACT ? 1 : kWarps][EXACT ? 1 : 32 * 4];     // [lane * 4 + k]
 };
 
 // One backprojection work unit: brick `brick` (brick order) of the volume,
@@ -237,6 +244,21 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
 #pragma unroll
     for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
 
+    // Fast modes: voxel-views the branch-free pass cannot finish (near-tie
+    // pixel choices, the detector-edge taper band; ~0.1-1 % of them) are not
+    // finished by their own lane -- that would stall the other 31 lanes of
+    // the warp -- but queued per warp as (view, voxel, lane) and finished 32
+    // at a time, every lane on a different item, whenever 32 are queued and
+    // at the end of each view chunk. Their contributions are summed per
+    // (lane, voxel) in shared memory and added to the accumulators at the end.
+    uint16_t *q = sm.q[EXACT ? 0 : warp];
+    float *qd = sm.qd[EXACT ? 0 : warp];
+    int qn = 0;
+    if constexpr (!EXACT) {
+#pragma unroll
+        for (int k = 0; k < kXB; ++k) qd[lane * 4 + k] = 0.f;
+    }
+
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
     const bool needZ = P.pL != 0 || P.pV != 0;
     const int n_sub = P.ssx * P.ssy * P.ssz;
@@ -247,6 +269,71 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                 const float fsub[3] = {-0.5f + offx * (0.5f + si), -0.5f + offy * (0.5f + sj),
                                        -0.5f + offz * (0.5f + sk)};
                 const float X0 = base[0] + fsub[0] * vw, Y0 = base[1] + fsub[1] * vw, Z0 = base[2] + fsub[2] * vw;
+
+                // Finish the first c queued items (lane j takes item j) with the
+                // full rule, then drop them from the queue. Warp-uniform call.
+                auto flush = [&](int c, uint32_t v0) {
+                    if (lane < c) {
+                        const unsigned e = q[lane];
+                        const int L = (int)(e & 31u), k = (int)((e >> 5) & 3u), tt = (int)(e >> 7);
+                        // the owner's voxel (same formulas as its own pass)
+                        int id[3];
+                        id[a0] = b0 * 32 + L;
+                        id[a1] = i1;
+                        id[a2] = i2b;
+                        float bb[3];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) bb[a] = ((float)id[a] + 0.5f - 0.5f * (float)P.n[a]) * vw;
+                        const float X = bb[0] + fsub[0] * vw, Y = bb[1] + fsub[1] * vw, Z = bb[2] + fsub[2] * vw;
+                        const ab_bpview bq = sv[tt];
+                        const float *pvq = P.projs + (int64_t)(v0 + tt) * P.stride_view;
+                        const float kf = (float)k;
+                        const float D = fmaf(kf, (a2 == 0 ? bq.den.x : (a2 == 1 ? bq.den.y : bq.den.z)) * vw,
+                                             dot4(bq.den, X, Y, Z));
+                        const float rD = rcp_fast(D);
+                        const float fu = fmaf(kf, (a2 == 0 ? bq.nu.x : (a2 == 1 ? bq.nu.y : bq.nu.z)) * vw,
+                                              dot4(bq.nu, X, Y, Z)) * rD;
+                        const float fv = fmaf(kf, (a2 == 0 ? bq.nv.x : (a2 == 1 ? bq.nv.y : bq.nv.z)) * vw,
+                                              dot4(bq.nv, X, Y, Z)) * rD;
+                        float w = RAYCAST ? 1.f : bq.kfast * rD * rD;
+                        if (needZ)
+                            w *= zpow(P, bq, fmaf(kf, (a2 == 0 ? bq.zl.x : (a2 == 1 ? bq.zl.y : bq.zl.z)) * vw,
+                                                  dot4(bq.zl, X, Y, Z)));
+                        float pv;
+                        if (BILIN) {
+                            pv = fetch_bilinear(P, pvq, fu, fv);
+                        } else {
+                            float du, dv;
+                            int iu = round_index(fu, -2.f, P.fnu1, du);
+                            int iv = round_index(fv, -2.f, P.fnv1, dv);
+                            const bool tu = fabsf(du) > bq.tie_u, tv = fabsf(dv) > bq.tie_v;
+                            if (tu || tv) {
+                                id[a2] = i2b + k;
+                                const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
+                                const ab_bpview_d &cd = svd[kNear ? tt : 0];
+                                if (tu) iu = refine_index(cd.nu, cd.den, vr, iu, du);
+                                if (tv) iv = refine_index(cd.nv, cd.den, vr, iv, dv);
+                            }
+                            const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
+                            pv = inb ? __ldg(pvq + (iu * P.su + iv * P.sv)) : 0.f;
+                        }
+                        float s = pv * w;
+                        if (P.sep > 0.f && s != 0.f) s *= taper(bq, fu, fv, P.inv_sep);
+                        atomicAdd(&qd[L * 4 + k], s);
+                    }
+                    __syncwarp();
+                    const int rem = qn - c;
+                    for (int i0q = 0; i0q < rem; i0q += 32) {
+                        const int i = i0q + lane;
+                        const uint16_t v = i < rem ? q[i + c] : (uint16_t)0;
+                        __syncwarp();
+                        if (i < rem) q[i] = v;
+                        __syncwarp();
+                    }
+                    qn = rem;
+                };
 
                 for (uint32_t v0 = 0; v0 < P.n_views; v0 += kChunk) {
                     const int cn = (int)min((uint32_t)kChunk, P.n_views - v0);
@@ -264,7 +351,8 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
                     }
                     __syncthreads();
-                    if (!any_live) continue;
+                    // warp-uniform skip (the fast modes' queue uses whole-warp votes)
+                    if (!__any_sync(0xffffffffu, any_live)) continue;
                     for (int t = 0; t < cn; ++t) {
                         const int view = (int)v0 + t;
                         const ab_bpview b = sv[t];
@@ -404,50 +492,32 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                 acc[k] = fmaf(pv, w, acc[k]);
                                 pending |= (live[k] && !fast) ? 1u << k : 0u;
                             }
-                            if (pending != 0u) {
+                            if (__any_sync(0xffffffffu, pending != 0u)) {
 #pragma unroll
                                 for (int k = 0; k < kXB; ++k) {
-                                    if (!((pending >> k) & 1u)) continue;
-                                    const float kf = (float)k;
-                                    const float D = fmaf(kf, dD, D0);
-                                    const float rD = rcp_fast(D);
-                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
-                                    const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                    float w = RAYCAST ? 1.f : b.kfast * rD * rD;
-                                    if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
-                                    float pv;
-                                    if (BILIN) {
-                                        pv = fetch_bilinear(P, pvw, fu, fv);
-                                    } else {
-                                        float du, dv;
-                                        int iu = round_index(fu, -2.f, P.fnu1, du);
-                                        int iv = round_index(fv, -2.f, P.fnv1, dv);
-                                        const bool tu = fabsf(du) > b.tie_u, tv = fabsf(dv) > b.tie_v;
-                                        if (tu || tv) {
-                                            int id[3];
-                                            id[a0] = i0;
-                                            id[a1] = i1;
-                                            id[a2] = i2b + k;
-                                            const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
-                                                            ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
-                                                            ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
-                                            const ab_bpview_d &c = svd[kNear ? t : 0];
-                                            if (tu) iu = refine_index(c.nu, c.den, vr, iu, du);
-                                            if (tv) iv = refine_index(c.nv, c.den, vr, iv, dv);
-                                        }
-                                        const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
-                                        pv = inb ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
-                                    }
-                                    float s = pv * w;
-                                    if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
-                                    acc[k] += s;
+                                    const bool p = (pending >> k) & 1u;
+                                    const unsigned m = __ballot_sync(0xffffffffu, p);
+                                    if (p) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint16_t)((t << 7) | (k << 5) | lane);
+                                    qn += __popc(m);
                                 }
+                                __syncwarp();
+                                while (qn >= 32) flush(32, v0);
                             }
                         }
+                    }
+                    // the queue refers to this chunk's coefficients: finish it now
+                    if constexpr (!EXACT) {
+                        if (qn > 0) flush(qn, v0);
                     }
                 }
             }
         }
+    }
+
+    if constexpr (!EXACT) {  // the deferred contributions (all sub-samples)
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < kXB; ++k) acc[k] += qd[lane * 4 + k];
     }
 
 #pragma unroll
