@@ -55,6 +55,11 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         ],
     ),
     "aprict_b200_forbild_compile": (_c_int, [_c_void_p, ctypes.c_int64, _c_void_p]),
+    "aprict_b200_sirt_step": (_c_int, [_c_void_p] * 9 + [_c_void_p]),
+    "aprict_b200_sirt_graph_create": (_c_int, [_c_void_p] * 9 + [_c_int, _c_void_p]),
+    "aprict_b200_sirt_graph_launch": (_c_int, [_c_void_p, _c_void_p]),
+    "aprict_b200_sirt_graph_iterations": (_c_int, [_c_void_p]),
+    "aprict_b200_sirt_graph_destroy": (None, [_c_void_p]),
     "aprict_b200_batch_plan_bytes": (ctypes.c_size_t, [_c_int, _c_int]),
     "aprict_b200_batch_plan": (_c_int, [_c_int, _c_void_p, _c_int, _c_void_p, _c_void_p, ctypes.c_size_t]),
     "aprict_b200_batch_run": (_c_int, [_c_void_p, _c_void_p, _c_void_p]),

@@ -298,6 +298,31 @@ APRICT_API int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
                                            float multiply_before_adding, uint32_t ssu, uint32_t ssv, int mode,
                                            uint32_t *overflow_dev, uint32_t *status_dev, aprict_stream_t stream);
 
+/* ---- SIRT (reference mode) ----
+ * One iteration of SIRT_flatpanel (sirt_vram.py:130-152) as two launches on
+ * the stream: r = b - A x (fused residual), then x += M (.) B r with cfg_bp
+ * (which must apply the summand multiplier M). b, r: projection stacks with
+ * the layout of pd; x, M: volumes of vd. */
+APRICT_API int aprict_b200_sirt_step(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                     const float *b_dev, float *r_dev, const aprict_vol_desc *vd, float *x_dev,
+                                     const float *M_dev, const aprict_backproject_config *cfg_bp,
+                                     uint32_t *status_dev, aprict_stream_t stream);
+
+/* n_iter SIRT steps captured once as a CUDA graph (on a private stream) and
+ * replayed with aprict_b200_sirt_graph_launch. The graph records the
+ * pointers and settings given here. The kernels must already be loaded when
+ * it is created: run one aprict_b200_sirt_step (or any projection and
+ * backprojection) in the process first. */
+typedef struct aprict_sirt_graph aprict_sirt_graph;
+APRICT_API int aprict_b200_sirt_graph_create(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                             const float *b_dev, float *r_dev, const aprict_vol_desc *vd,
+                                             float *x_dev, const float *M_dev,
+                                             const aprict_backproject_config *cfg_bp, uint32_t *status_dev,
+                                             int n_iter, aprict_sirt_graph **out);
+APRICT_API int aprict_b200_sirt_graph_launch(const aprict_sirt_graph *graph, aprict_stream_t stream);
+APRICT_API int aprict_b200_sirt_graph_iterations(const aprict_sirt_graph *graph);
+APRICT_API void aprict_b200_sirt_graph_destroy(aprict_sirt_graph *graph);
+
 /* ---- Many scans in one persistent launch ----
  * No reference counterpart (the reference runs one scan per call). A batch is
  * a plan built on the host from per-scan arguments -- exactly the arguments

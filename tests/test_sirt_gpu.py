@@ -150,3 +150,40 @@ def test_landweber_ordered_subsets() -> None:
     r = fp.ProjectionSet(pg, data=None)
     fp.project_residual(fp.ConfigProject(multiply_before_adding=-1), x, r, b)
     assert float(torch.linalg.vector_norm(r.data)) < 0.5 * r0
+
+
+def test_c_abi_sirt_step_and_graph_equal_the_python_iterator() -> None:
+    """aprict_b200_sirt_step / sirt_graph_* (the C entry points) against SIRT_flatpanel."""
+    import ctypes
+
+    from aprict_b200 import _lib
+
+    pg, _, b = _problem()
+    sa = SIRT_flatpanel(SIRT_flatpanel.Config(), Volume.zeros(SHAPE, voxwid=1.0), fp.ProjectionSet(pg, data=b.clone()))
+    sb = SIRT_flatpanel(SIRT_flatpanel.Config(), Volume.zeros(SHAPE, voxwid=1.0), fp.ProjectionSet(pg, data=b.clone()))
+    lib = _lib.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    meas, r, x, M = sb._meas, sb._scratch, sb.volume, sb.preconditioner  # noqa: SLF001
+    pd = _lib.proj_desc(tuple(r.data.shape), tuple(r.data.stride()))
+    vd = x._desc()  # noqa: SLF001
+    cfg = sb._config_bp.contents  # noqa: SLF001
+    args = (meas.specs_device().data_ptr(), _lib.ptr(pd), meas.data.data_ptr(), r.data.data_ptr(), _lib.ptr(vd),
+            x.data.data_ptr(), M.data.data_ptr(), _lib.ptr(cfg), None)
+    for _ in range(2):
+        sa.iterate()
+        _lib.check(lib.aprict_b200_sirt_step(*args, stream), "sirt_step")
+    torch.cuda.synchronize()
+    assert torch.equal(sa.volume.data, x.data)
+    g = ctypes.c_void_p()
+    _lib.check(lib.aprict_b200_sirt_graph_create(*args, 3, ctypes.byref(g)), "sirt_graph_create")
+    try:
+        assert lib.aprict_b200_sirt_graph_iterations(g) == 3
+        _lib.check(lib.aprict_b200_sirt_graph_launch(g, stream), "sirt_graph_launch")
+        for _ in range(3):
+            sa.iterate()
+        torch.cuda.synchronize()
+        assert rel_l2(x.as_numpy(), sa.volume.as_numpy()) <= 1e-6
+    finally:
+        lib.aprict_b200_sirt_graph_destroy(g)
+    with pytest.raises(ValueError):
+        _lib.check(lib.aprict_b200_sirt_step(*args[:6], None, _lib.ptr(cfg), None, stream), "sirt_step")
