@@ -237,12 +237,8 @@ AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3
 #pragma unroll 2
     for (;;) {
         const float tm = fminf(tx, fminf(ty, tz));
-        const float seg = fminf(tm, R.tend) - t;
-        if (tm >= R.tend) {
-            const float y = seg * mu - c;
-            s += y;
-            break;
-        }
+        if (tm >= R.tend) break;
+        const float seg = tm - t;
         t = tm;
         AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm);
         const float mu_next = load(off);  // in the grid: the loop did not stop
@@ -252,6 +248,7 @@ AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3
         s = tt;
         mu = mu_next;
     }
+    s += (R.tend - t) * mu - c;  // the last segment ends at the exit
     sum = s;
     return true;
 }
