@@ -55,6 +55,12 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
         ],
     ),
     "aprict_b200_forbild_compile": (_c_int, [_c_void_p, ctypes.c_int64, _c_void_p]),
+    "aprict_b200_forbild_sample": (
+        _c_int,
+        [_c_void_p, ctypes.c_int64, _c_void_p, _c_void_p, _c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+         ctypes.c_uint32, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _c_void_p, ctypes.c_float,
+         ctypes.c_uint32, _c_void_p],
+    ),
     "aprict_b200_sirt_step": (_c_int, [_c_void_p] * 9 + [_c_void_p]),
     "aprict_b200_sirt_graph_create": (_c_int, [_c_void_p] * 9 + [_c_int, _c_void_p]),
     "aprict_b200_sirt_graph_launch": (_c_int, [_c_void_p, _c_void_p]),

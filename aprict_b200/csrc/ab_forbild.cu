@@ -265,10 +265,12 @@ extern "C" int aprict_b200_forbild_compile(const aprict_forbild_shape *sh, int64
         for (int k = 0; k < 3; ++k) {
             if (cs[k]->mode == 0) continue;
             const double sg = cs[k]->mode == 1 ? 1.0 : -1.0;  // mode 2 keeps a.p > d
-            q.clip[q.n_clip][0] = sg * cs[k]->axis.x;
-            q.clip[q.n_clip][1] = sg * cs[k]->axis.y;
-            q.clip[q.n_clip][2] = sg * cs[k]->axis.z;
-            q.clip[q.n_clip][3] = sg * cs[k]->dotprod;
+            const int kc = q.n_clip & 0xFF;
+            q.clip[kc][0] = sg * cs[k]->axis.x;
+            q.clip[kc][1] = sg * cs[k]->axis.y;
+            q.clip[kc][2] = sg * cs[k]->axis.z;
+            q.clip[kc][3] = sg * cs[k]->dotprod;
+            if (cs[k]->mode == 2) q.n_clip |= 0x100 << kc;  // strict: a.p > d
             q.n_clip++;
         }
         out[i] = q;
@@ -335,7 +337,7 @@ __device__ void make_qview(const ViewGeom &g, const aprict_quadric &q, QView &o)
     mul(g.U, o.du);
     mul(g.V, o.dv);
     o.kind = q.kind;
-    o.n_clip = q.n_clip;
+    o.n_clip = q.n_clip & 0xFF;
     o.rho = q.rho;
     o.h = q.h;
     o.alpha = q.alpha;
@@ -347,7 +349,7 @@ __device__ void make_qview(const ViewGeom &g, const aprict_quadric &q, QView &o)
     else
         o.cq = 0.0;
     for (int k = 0; k < 3; ++k) {
-        if (k < q.n_clip) {
+        if (k < (q.n_clip & 0xFF)) {
             const ab_d3 a{q.clip[k][0], q.clip[k][1], q.clip[k][2]};
             o.g0[k] = ab_dot(a, g.s) - q.clip[k][3];
             o.gd0[k] = ab_dot(a, g.D0);
@@ -643,4 +645,154 @@ extern "C" int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
         if (rc != APRICT_OK) return rc;
     }
     return APRICT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Point sampling ("last shape wins") -- replaces add_FORBILD_sampling
+// (src/aprict/data/cusrc/sample_FORBILD_volumes.cu:10-123): per voxel and
+// sub-sample the value is the density of the last shape (in order) that
+// contains the point, 0 if none; the mean over the sub-samples is added to
+// the output. Each CTA (an 8 x 8 x 4 voxel block) first keeps, in order, the
+// shapes whose bounding boxes meet its own box, 256 at a time.
+
+namespace {
+
+// Closed solids, as the reference's _in_region (FORBILD_volumes.h); the
+// strict clip planes (">") exclude their plane.
+__device__ __forceinline__ bool in_quadric(const aprict_quadric &q, double px, double py, double pz) {
+    const int nc = q.n_clip & 0xFF;
+    for (int k = 0; k < nc; ++k) {
+        const double g = q.clip[k][0] * px + q.clip[k][1] * py + q.clip[k][2] * pz - q.clip[k][3];
+        if ((q.n_clip >> (8 + k)) & 1 ? !(g < 0.0) : !(g <= 0.0)) return false;
+    }
+    const double dx = px - q.c[0], dy = py - q.c[1], dz = pz - q.c[2];
+    const double lx = q.M[0] * dx + q.M[1] * dy + q.M[2] * dz;
+    const double ly = q.M[3] * dx + q.M[4] * dy + q.M[5] * dz;
+    const double lz = q.M[6] * dx + q.M[7] * dy + q.M[8] * dz;
+    switch (q.kind) {
+        case 1: return lx * lx + ly * ly + lz * lz <= 1.0;
+        case 2: return fabs(lz) <= q.h && lx * lx + ly * ly <= 1.0;
+        case 3: {
+            const double r = q.alpha + q.beta * lz;
+            return fabs(lz) <= q.h && lx * lx + ly * ly <= r * r;
+        }
+        case 4: return fabs(lx) <= 1.0 && fabs(ly) <= 1.0 && fabs(lz) <= 1.0;
+        default: return false;
+    }
+}
+
+constexpr int kSampleThreads = 256;  // 8 (x) x 8 (y) x 4 (z) voxels
+
+__global__ void __launch_bounds__(kSampleThreads) k_forbild_sample(const aprict_quadric *__restrict__ shapes, int n,
+                                                                    const float *__restrict__ xs,
+                                                                    const float *__restrict__ ys,
+                                                                    const float *__restrict__ zs, int nx, int ny,
+                                                                    int nz, int64_t sx, int64_t sy, int64_t sz,
+                                                                    float *out, float ss_wid, int ss) {
+    __shared__ int keep[kSampleThreads];
+    __shared__ int nkeep;
+    __shared__ float box[6];  // CTA box: min x y z, max x y z
+    const int t = threadIdx.x;
+    const int bx = blockIdx.x * 8, by = blockIdx.y * 8, bz = blockIdx.z * 4;
+    const int ix = bx + (t & 7), iy = by + ((t >> 3) & 7), iz = bz + (t >> 6);
+    const bool inr = ix < nx && iy < ny && iz < nz;
+    // The block's box from its coordinates (grids need not be monotonic).
+    if (t < 32) {
+        const int lane = t;
+        float lo[3], hi[3];
+        const float *arr[3] = {xs, ys, zs};
+        const int b0[3] = {bx, by, bz}, ext[3] = {8, 8, 4}, nn[3] = {nx, ny, nz};
+        for (int a = 0; a < 3; ++a) {
+            const int i = b0[a] + (lane % ext[a]);
+            const float v = i < nn[a] ? arr[a][i] : arr[a][b0[a]];
+            float mn = v, mx = v;
+            for (int o = 16; o > 0; o >>= 1) {
+                mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            lo[a] = mn;
+            hi[a] = mx;
+        }
+        if (lane == 0) {
+            const float hw = 0.5f * ss_wid;
+            for (int a = 0; a < 3; ++a) {
+                box[a] = lo[a] - hw;
+                box[3 + a] = hi[a] + hw;
+            }
+        }
+    }
+    const double cx = inr ? (double)xs[ix] : 0.0, cy = inr ? (double)ys[iy] : 0.0, cz = inr ? (double)zs[iz] : 0.0;
+    float total = 0.f;
+    for (int s = 0; s < ss * ss * ss; ++s) {
+        const int ox = s / (ss * ss), oy = (s / ss) % ss, oz = s % ss;
+        const double px = cx + ((ox - 0.5 * (ss - 1)) / ss) * (double)ss_wid;
+        const double py = cy + ((oy - 0.5 * (ss - 1)) / ss) * (double)ss_wid;
+        const double pz = cz + ((oz - 0.5 * (ss - 1)) / ss) * (double)ss_wid;
+        float val = 0.f;
+        for (int base = 0; base < n; base += kSampleThreads) {
+            __syncthreads();  // box ready; the previous chunk's list is consumed
+            const int j = base + t;
+            bool meet = false;
+            if (j < n && shapes[j].kind != 0) {
+                const aprict_quadric &q = shapes[j];
+                meet = true;
+                for (int a = 0; a < 3; ++a)
+                    meet = meet && q.c[a] - q.bb_half[a] <= (double)box[3 + a] && q.c[a] + q.bb_half[a] >= (double)box[a];
+            }
+            // ordered compaction: warp ballots, then warp offsets
+            const unsigned bal = __ballot_sync(0xffffffffu, meet);
+            __shared__ int wcount[kSampleThreads / 32];
+            if ((t & 31) == 0) wcount[t >> 5] = __popc(bal);
+            __syncthreads();
+            if (meet) {
+                int off = __popc(bal & ((1u << (t & 31)) - 1u));
+                for (int w = 0; w < (t >> 5); ++w) off += wcount[w];
+                keep[off] = j;
+            }
+            if (t == 0) {
+                int c = 0;
+                for (int w = 0; w < kSampleThreads / 32; ++w) c += wcount[w];
+                nkeep = c;
+            }
+            __syncthreads();
+            if (inr) {
+                const int c = nkeep;
+                for (int i = 0; i < c; ++i) {
+                    const aprict_quadric &q = shapes[keep[i]];
+                    if (in_quadric(q, px, py, pz)) val = (float)q.rho;
+                }
+            }
+        }
+        total += val;
+    }
+    if (!inr || total == 0.f) return;
+    total /= (float)(ss * ss * ss);
+    atomicAdd(out + (int64_t)ix * sx + (int64_t)iy * sy + (int64_t)iz * sz, total);
+}
+
+}  // namespace
+
+extern "C" int aprict_b200_forbild_sample(const aprict_quadric *shapes_dev, int64_t n_shapes, const float *xs_dev,
+                                          const float *ys_dev, const float *zs_dev, uint32_t nx, uint32_t ny,
+                                          uint32_t nz, int64_t stride_x, int64_t stride_y, int64_t stride_z,
+                                          float *out_dev, float supersamp_voxwid, uint32_t supersamp_factor,
+                                          aprict_stream_t stream) {
+    if (n_shapes < 0 || n_shapes > (1 << 24)) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "bad shape count");
+    if (supersamp_factor == 0 || supersamp_factor > 8)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "supersamp_factor must be in [1, 8]");
+    if (!isfinite(supersamp_voxwid) || supersamp_voxwid < 0.f)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "supersamp_cubic_vox_wid must be finite and >= 0");
+    if (nx == 0 || ny == 0 || nz == 0 || n_shapes == 0) return APRICT_OK;
+    if (nx > (1u << 30) || ny > (1u << 30) || nz > (1u << 30))
+        return ab_fail(APRICT_ERR_TOO_LARGE, "forbild_sample: grid edge exceeds 2^30");
+    if (shapes_dev == nullptr || xs_dev == nullptr || ys_dev == nullptr || zs_dev == nullptr || out_dev == nullptr)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "forbild_sample: null pointer");
+    if (stride_x < 0 || stride_y < 0 || stride_z < 0)
+        return ab_fail(APRICT_ERR_UNSUPPORTED, "forbild_sample: negative strides are not supported");
+    const dim3 grid((nx + 7) / 8, (ny + 7) / 8, (nz + 3) / 4);
+    if (grid.y > 65535u || grid.z > 65535u) return ab_fail(APRICT_ERR_TOO_LARGE, "forbild_sample: grid too large");
+    k_forbild_sample<<<grid, kSampleThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        shapes_dev, (int)n_shapes, xs_dev, ys_dev, zs_dev, (int)nx, (int)ny, (int)nz, stride_x, stride_y, stride_z,
+        out_dev, supersamp_voxwid, (int)supersamp_factor);
+    return ab_cuda_check(cudaGetLastError(), "forbild_sample launch");
 }

@@ -10,6 +10,8 @@ the kernels index directly. Voxel centres follow the reference convention:
 
 from __future__ import annotations
 
+import os
+
 import pathlib
 import typing
 
@@ -382,6 +384,131 @@ class FBVolume:
     def superimpose_onto(self, vol: FBVolume) -> FBVolume:
         """This phantom's shapes drawn after (over) ``vol``'s."""
         return FBVolume(shapes=np.concatenate((vol.shapes, self.shapes), axis=0))
+
+    # ------------------------------------------------------------- files
+    @classmethod
+    def load(cls, path_to_pha: str | os.PathLike) -> FBVolume:
+        """Read a ``.pha`` phantom file (volume.py:388-390)."""
+        from . import pha  # noqa: PLC0415
+
+        return cls(pha.load(path_to_pha))
+
+    @property
+    def FORBILD_str(self) -> str:  # noqa: N802
+        """The phantom in .pha syntax (volume.py:383-386)."""
+        from . import pha  # noqa: PLC0415
+
+        return pha.format_shapes(self.shapes)
+
+    def save(self, path_to_pha: str | os.PathLike) -> None:
+        """Write the phantom as a ``.pha`` file (volume.py:392-395)."""
+        with open(path_to_pha, mode="w", encoding="utf-8") as f:
+            f.write(self.FORBILD_str)
+
+    # ---------------------------------------------------------- sampling
+    def to_tensor(
+        self,
+        xs: np.ndarray,
+        ys: np.ndarray,
+        zs: np.ndarray,
+        *,
+        out: torch.Tensor | None = None,
+        supersamp_cubic_vox_wid: float | None = None,
+        supersamp_factor: int | None = None,
+        block: bool = True,
+    ) -> torch.Tensor:
+        """Point-sample the phantom onto the grid ``xs x ys x zs``, "last shape
+        wins", averaging ``supersamp_factor``^3 sub-samples spread over a cube
+        of edge ``supersamp_cubic_vox_wid`` per voxel; the result is ADDED to
+        ``out`` (float32 CUDA tensor (len(xs), len(ys), len(zs)), new and
+        zeroed if None) -- the reference's to_cupy (volume.py:397-418,
+        sample_FORBILD_volumes.cu:10-123)."""
+        from .cb import forbild  # noqa: PLC0415
+        from .cb.flatpanel import _device, _stream  # noqa: PLC0415
+
+        dev = _device()
+        axes = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev) for a in (xs, ys, zs)]
+        shape = tuple(int(a.numel()) for a in axes)
+        if out is None:
+            out = torch.zeros(shape, dtype=torch.float32, device=dev)
+        elif tuple(out.shape) != shape or out.dtype != torch.float32 or not out.is_cuda:
+            msg = f"out must be a float32 CUDA tensor of shape {shape}"
+            raise ValueError(msg)
+        ss = int(supersamp_factor or 1)
+        wid = float(supersamp_cubic_vox_wid or 0.0)
+        if ss > 1 and wid <= 0.0:
+            msg = "supersampling needs supersamp_cubic_vox_wid > 0"
+            raise ValueError(msg)
+        comp = forbild._compiled(self)  # noqa: SLF001
+        if comp.n > 0 and comp.dev is not None:
+            _lib.check(
+                _lib.lib().aprict_b200_forbild_sample(
+                    comp.dev.data_ptr(), comp.n, axes[0].data_ptr(), axes[1].data_ptr(), axes[2].data_ptr(),
+                    shape[0], shape[1], shape[2], *out.stride(), out.data_ptr(), wid, ss, _stream(),
+                ),
+                "forbild_sample",
+            )
+        if block:
+            torch.cuda.current_stream().synchronize()
+        return out
+
+    def to_numpy(self, xs: np.ndarray, ys: np.ndarray, zs: np.ndarray, **kw) -> np.ndarray:
+        """:meth:`to_tensor` copied to the host (volume.py:503-508)."""
+        return self.to_tensor(xs, ys, zs, **kw).cpu().numpy()
+
+    def sample_into(self, volume: Volume, *, supersamp_factor: int = 1) -> Volume:
+        """Add the phantom, point-sampled at ``volume``'s voxel centres (with
+        ``supersamp_factor``^3 sub-samples per voxel), into ``volume``."""
+        xs, ys, zs = volume.xs_ys_zs
+        self.to_tensor(xs, ys, zs, out=volume.data, supersamp_cubic_vox_wid=volume.voxwid,
+                       supersamp_factor=supersamp_factor, block=False)
+        return volume
+
+    # -------------------------------------------------------- transforms
+    _LEN_KEYS = ("x", "y", "z", "r", "l", "dx", "dy", "dz", "r1", "r2")
+
+    def scale_len(self, factor: float) -> None:
+        """Scale every length (and clip offset) by ``factor`` (volume.py:510-537)."""
+        s = self.shapes.copy()
+        for k in self._LEN_KEYS:
+            s[k] *= np.float32(factor)
+        for c in ("cas1", "cas2", "cas3"):
+            s[c]["dotprod"] *= np.float32(factor)
+        self.shapes = s
+
+    @staticmethod
+    def _axis_name(axis: int | str) -> str:
+        names = {0: "x", 1: "y", 2: "z", "x": "x", "y": "y", "z": "z"}
+        if axis not in names:
+            msg = f"Unknown axis: {axis}"
+            raise ValueError(msg)
+        return names[axis]
+
+    def flip(self, axis: int | str) -> None:
+        """Mirror the phantom along one axis (volume.py:540-573)."""
+        a = self._axis_name(axis)
+        s = self.shapes.copy()
+        s[a] *= -1
+        for c in ("cas1", "cas2", "cas3"):
+            s[c]["axis"][a] *= -1
+        for v in ("axis", "a_x", "a_y", "a_z"):
+            s[v][a] *= -1
+        self.shapes = s
+
+    def translate(self, axis: int | str, amount: float) -> None:
+        """Move the phantom along one axis (volume.py:575-607)."""
+        a = self._axis_name(axis)
+        s = self.shapes.copy()
+        s[a] += np.float32(amount)
+        for c in ("cas1", "cas2", "cas3"):
+            s[c]["dotprod"] += np.float32(amount) * s[c]["axis"][a]
+        self.shapes = s
+
+    def multiply_attenuation(self, amount: float) -> None:
+        """Scale every density (volume.py:609-624)."""
+        s = self.shapes.copy()
+        s["rho"] *= np.float32(amount)
+        self.shapes = s
 
 
 __all__ = ["FBVolume", "Volume"]

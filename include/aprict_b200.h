@@ -264,7 +264,8 @@ typedef struct {
  *   kind 2: lx^2+ly^2 <= 1, |lz| <= h           (cylinders)
  *   kind 3: lx^2+ly^2 <= (alpha+beta lz)^2, |lz| <= h   (cone frusta)
  *   kind 4: |lx|,|ly|,|lz| <= 1                 (boxes)
- * clipped by g_k(p) = clip[k].xyz . p - clip[k].w <= 0 for k < n_clip. */
+ * clipped by g_k(p) = clip[k].xyz . p - clip[k].w <= 0 for k < (n_clip & 0xFF);
+ * bit 8 + k of n_clip marks clip k as strict (< 0: the FORBILD ">" planes). */
 typedef struct {
     int32_t kind;
     int32_t n_clip;
@@ -378,6 +379,18 @@ APRICT_API int aprict_b200_batch_run(const void *plan_host, void *plan_dev, apri
  * before any stream capture; calls that overlap in time on one device share
  * the array and race, so serialise them (one stream, or events). */
 APRICT_API int aprict_b200_batch_run_static(const void *plan_host, aprict_stream_t stream);
+
+/* Point-sample compiled shapes onto a grid, "last shape wins"
+ * (add_FORBILD_sampling, sample_FORBILD_volumes.cu:10-123): for voxel
+ * (i, j, k) at (xs[i], ys[j], zs[k]) and each of supersamp_factor^3
+ * sub-samples spaced supersamp_voxwid / supersamp_factor apart around it, the
+ * density of the last shape containing the point (0 if none); the mean is
+ * added to out[i*stride_x + j*stride_y + k*stride_z]. Entry tests in FP64. */
+APRICT_API int aprict_b200_forbild_sample(const aprict_quadric *shapes_dev, int64_t n_shapes, const float *xs_dev,
+                                          const float *ys_dev, const float *zs_dev, uint32_t nx, uint32_t ny,
+                                          uint32_t nz, int64_t stride_x, int64_t stride_y, int64_t stride_z,
+                                          float *out_dev, float supersamp_voxwid, uint32_t supersamp_factor,
+                                          aprict_stream_t stream);
 
 #ifdef __cplusplus
 }

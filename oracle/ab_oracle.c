@@ -674,3 +674,111 @@ void ao_project_forbild(const ao_proj_spec *specs, int n_views, int nu, int nv, 
         free(ev);
     }
 }
+
+/* ---- FORBILD point sampling (FP64), restating add_FORBILD_sampling
+ * (src/aprict/data/cusrc/sample_FORBILD_volumes.cu:10-123) with point tests
+ * in each shape's natural coordinates: closed solids, clip mode 1 keeps
+ * a.p <= d and mode 2 keeps a.p > d (as FORBILD_volumes.h:93-105). */
+int ao_forbild_inside(const double pw[3], const ao_forbild_shape *s) {
+    if (s->type == 0) return 0;
+    for (int k = 0; k < 3; ++k) {
+        const ao_clip *c = &s->cas[k];
+        if (c->mode == 0) continue;
+        const double a[3] = {c->axis.x, c->axis.y, c->axis.z};
+        const double g = dot3(a, pw);
+        if (c->mode == 1 ? !(g <= c->dotprod) : !(g > c->dotprod)) return 0;
+    }
+    const double p[3] = {pw[0] - s->x, pw[1] - s->y, pw[2] - s->z};
+    const double ex[3] = {1, 0, 0}, ey[3] = {0, 1, 0}, ez[3] = {0, 0, 1};
+    double ax[3], ay[3], az[3];
+    switch (s->type) {
+        case 13: return dot3(p, p) <= (double)s->r * s->r;
+        case 10: {
+            const double q[3] = {p[0] / s->dx, p[1] / s->dy, p[2] / s->dz};
+            return dot3(q, q) <= 1.0;
+        }
+        case 11: {
+            unit3(s->a_x, ax);
+            unit3(s->a_y, ay);
+            unit3(s->a_z, az);
+            const double q[3] = {dot3(p, ax) / s->dx, dot3(p, ay) / s->dy, dot3(p, az) / s->dz};
+            return dot3(q, q) <= 1.0;
+        }
+        case 12:
+        case 14:
+        case 15:
+        case 16: {
+            double sx, sy;
+            if (s->type == 12) {
+                unit3(s->a_x, ax);
+                unit3(s->a_y, ay);
+                unit3(s->axis, az);
+                sx = s->dx;
+                sy = s->dy;
+            } else {
+                const double *A = s->type == 14 ? ey : ex, *B = s->type == 16 ? ey : ez;
+                const double *C = s->type == 14 ? ex : (s->type == 15 ? ey : ez);
+                memcpy(ax, A, sizeof(ax));
+                memcpy(ay, B, sizeof(ay));
+                memcpy(az, C, sizeof(az));
+                sx = s->type == 14 ? s->dy : s->dx;
+                sy = s->type == 16 ? s->dy : s->dz;
+            }
+            const double u = dot3(p, ax) / sx, v = dot3(p, ay) / sy;
+            return fabs(dot3(p, az)) <= 0.5 * s->l && u * u + v * v <= 1.0;
+        }
+        case 6:
+        case 7:
+        case 8:
+        case 9: {
+            double a[3];
+            if (s->type == 6)
+                unit3(s->axis, a);
+            else
+                memcpy(a, s->type == 7 ? ex : (s->type == 8 ? ey : ez), sizeof(a));
+            const double z = dot3(p, a);
+            const double r2 = dot3(p, p) - z * z;
+            return fabs(z) <= 0.5 * s->l && r2 <= (double)s->r * s->r;
+        }
+        case 2:
+        case 3:
+        case 4:
+        case 5: {
+            double a[3];
+            if (s->type == 2)
+                unit3(s->axis, a);
+            else
+                memcpy(a, s->type == 3 ? ex : (s->type == 4 ? ey : ez), sizeof(a));
+            const double z = dot3(p, a);
+            if (!(fabs(z) <= 0.5 * s->l)) return 0;
+            const double r = 0.5 * ((double)s->r1 + s->r2) + ((double)s->r2 - s->r1) / s->l * z;
+            return dot3(p, p) - z * z <= r * r;
+        }
+        case 1: return fabs(p[0]) <= 0.5 * s->dx && fabs(p[1]) <= 0.5 * s->dy && fabs(p[2]) <= 0.5 * s->dz;
+        default: return 0;
+    }
+}
+
+void ao_forbild_sample(const ao_forbild_shape *shapes, int n, const double *xs, const double *ys, const double *zs,
+                       int nx, int ny, int nz, double ss_wid, int ss, double *out, int nthreads) {
+#pragma omp parallel for collapse(2) schedule(dynamic, 4) num_threads(nthreads)
+    for (int i = 0; i < nx; ++i) {
+        for (int j = 0; j < ny; ++j) {
+            for (int k = 0; k < nz; ++k) {
+                double tot = 0.0;
+                for (int a = 0; a < ss; ++a)
+                    for (int b = 0; b < ss; ++b)
+                        for (int c = 0; c < ss; ++c) {
+                            const double p[3] = {xs[i] + (a - 0.5 * (ss - 1)) / ss * ss_wid,
+                                                 ys[j] + (b - 0.5 * (ss - 1)) / ss * ss_wid,
+                                                 zs[k] + (c - 0.5 * (ss - 1)) / ss * ss_wid};
+                            double val = 0.0;
+                            for (int m = 0; m < n; ++m)
+                                if (ao_forbild_inside(p, &shapes[m])) val = shapes[m].rho;
+                            tot += val;
+                        }
+                out[((size_t)i * ny + j) * nz + k] = tot / ((double)ss * ss * ss);
+            }
+        }
+    }
+}

@@ -71,5 +71,8 @@ void ao_project_forbild(const ao_proj_spec *specs, int n_views, int nu, int nv, 
 
 /* Interval [t0,t1] of the segment v1->v2 with one shape (after clipping), FP64. */
 int ao_forbild_interval(const double v1[3], const double v2[3], const ao_forbild_shape *s, double out2[2]);
+int ao_forbild_inside(const double p[3], const ao_forbild_shape *s);
+void ao_forbild_sample(const ao_forbild_shape *shapes, int n, const double *xs, const double *ys, const double *zs,
+                       int nx, int ny, int nz, double ss_wid, int ss, double *out, int nthreads);
 
 #endif

@@ -372,3 +372,27 @@ def ref_forbild_interval(v1: np.ndarray, v2: np.ndarray, shape: np.ndarray) -> t
     sh = np.ascontiguousarray(shape.reshape(1))
     lib.ref_forbild_interval(_p(a), _p(b), _p(sh), _p(o))
     return float(o[0]), float(o[1])
+
+
+def forbild_sample(shapes: np.ndarray, xs, ys, zs, *, ss_wid: float = 0.0, ss: int = 1,
+                   nthreads: int | None = None) -> np.ndarray:
+    """FP64 "last shape wins" point sampling (natural-coordinate point tests)."""
+    lib = _load(ORACLE_SO)
+    ax = [np.ascontiguousarray(a, np.float64) for a in (xs, ys, zs)]
+    sh = np.ascontiguousarray(shapes.reshape(-1))
+    out = np.zeros((len(ax[0]), len(ax[1]), len(ax[2])), np.float64)
+    lib.ao_forbild_sample(_p(sh), len(sh), _p(ax[0]), _p(ax[1]), _p(ax[2]), len(ax[0]), len(ax[1]), len(ax[2]),
+                          ctypes.c_double(ss_wid), ss, _p(out), nthreads or nthreads_default())
+    return out
+
+
+def ref_forbild_sample(shapes: np.ndarray, xs, ys, zs, *, ss_wid: float = 0.0, ss: int = 1,
+                       nthreads: int | None = None) -> np.ndarray:
+    """The reference's sampling body (its own _in_region, FP32) on the CPU."""
+    lib = _load(REF_SO)
+    ax = [np.ascontiguousarray(a, np.float32) for a in (xs, ys, zs)]
+    sh = np.ascontiguousarray(shapes.reshape(-1))
+    out = np.zeros((len(ax[0]), len(ax[1]), len(ax[2])), np.float32)
+    lib.ref_forbild_sample(_p(sh), len(sh), _p(ax[0]), _p(ax[1]), _p(ax[2]), len(ax[0]), len(ax[1]), len(ax[2]),
+                           ctypes.c_float(ss_wid), ss, _p(out), nthreads or nthreads_default())
+    return out

@@ -141,6 +141,38 @@ void ref_forbild_bbox(const void *shape, float *out6) {
     out6[5] = b.xyz_max.z;
 }
 
+// The per-voxel body of add_FORBILD_sampling (sample_FORBILD_volumes.cu:28-122)
+// restated on the CPU around the reference's own _in_region(fvec3,
+// FORBILD_Shape) (FORBILD_volumes.h:1626-): for each sub-sample the density
+// of the last shape containing the point, the mean over sub-samples (the
+// kernel's offsets, including its y <- offz, z <- offy order).
+void ref_forbild_sample(const void *shapes, unsigned n, const float *xs, const float *ys, const float *zs,
+                        unsigned nx, unsigned ny, unsigned nz, float ss_wid, unsigned ss, float *out, int nthreads) {
+    const refp::FORBILD_Shape *sh = (const refp::FORBILD_Shape *)shapes;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4) num_threads(nthreads)
+    for (unsigned i = 0; i < nx; ++i) {
+        for (unsigned j = 0; j < ny; ++j) {
+            for (unsigned k = 0; k < nz; ++k) {
+                const refp::fvec3 pos_c(xs[i], ys[j], zs[k]);
+                float totval = 0.f;
+                for (unsigned ox = 0; ox < ss; ++ox)
+                    for (unsigned oy = 0; oy < ss; ++oy)
+                        for (unsigned oz = 0; oz < ss; ++oz) {
+                            const refp::fvec3 pos = pos_c + refp::fvec3((ox - (ss - 1.f) / 2.f) / (float)ss,
+                                                                        (oz - (ss - 1.f) / 2.f) / (float)ss,
+                                                                        (oy - (ss - 1.f) / 2.f) / (float)ss) *
+                                                                ss_wid;
+                            float val = 0.f;
+                            for (unsigned m = 0; m < n; ++m)
+                                if (refp::_in_region(pos, sh[m])) val = sh[m].rho;
+                            totval += val;
+                        }
+                out[((size_t)i * ny + j) * nz + k] = totval == 0.f ? 0.f : totval / (float)(ss * ss * ss);
+            }
+        }
+    }
+}
+
 unsigned ref_sizeof_proj_spec(void) { return sizeof(refp::proj_spec); }
 unsigned ref_sizeof_forbild_shape(void) { return sizeof(refp::FORBILD_Shape); }
 }
