@@ -174,8 +174,8 @@ class ScanBatch:
                     raise ValueError(msg)
                 recs[i]["multiplier_dev"] = m.data.data_ptr()
                 keep.append(m)
-            if int(c.contents["weighting_preset"]) != 0:
-                msg = "Backprojection weighting presets 1-7 (cone-cylinder FBP / GBC) are not implemented."
+            if int(c.contents["weighting_preset"]) > 6:
+                msg = "Backprojection weighting preset 7 (the GBC formula) is not implemented."
                 raise NotImplementedError(msg)
         conf = _packed([c.contents for c in cfgs], S.backproject_config)
         return BatchPlan(BACKPROJECT, recs, conf, keep)

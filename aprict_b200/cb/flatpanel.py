@@ -631,8 +631,8 @@ def backproject(
     if bool(cfg["apply_summand_multiplier"]) != (summand_multiplier is not None):
         msg = "To prevent unintended behaviour, the config 'apply_summand_multiplier' must be true if and only if a summand_multiplier is included."
         raise ValueError(msg)
-    if int(cfg["weighting_preset"]) != 0 or secondary_volume is not None:
-        msg = "Backprojection weighting presets 1-7 (cone-cylinder FBP / GBC) are not implemented."
+    if int(cfg["weighting_preset"]) > 6 or secondary_volume is not None:
+        msg = "Backprojection weighting preset 7 (the GBC formula, with its secondary volume) is not implemented."
         raise NotImplementedError(msg)
     _check_volume_device(volume)
     vd = volume._desc()  # noqa: SLF001

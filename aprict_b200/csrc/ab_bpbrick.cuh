@@ -59,6 +59,7 @@ struct BPParams {
     int pL, pV;
     float val;
     float inv_val;  // 1 / val
+    int preset;     // direct-raycast weighting preset 0-6
     int ssx, ssy, ssz;
     uint32_t *status;
 };
@@ -144,6 +145,28 @@ __device__ __forceinline__ float powi_fast(float x, int e) {
     float a = 1.f;
     for (int k = 0; k < n; ++k) a *= r;
     return a;
+}
+
+// Cone-cylinder weighting presets 1-6 of the direct-raycast mode
+// (CB_backproject.cu:530-599), R = val: xw, yw the voxel's world x, y; Z its
+// distance from the source along the source-detector axis.
+__device__ __forceinline__ float preset_weight(int preset, float R, float xw, float yw, float sx, float sy, float Z) {
+    const float rx = xw - sx, ry = yw - sy;
+    const float ell = sqrtf(rx * rx + ry * ry) / R;
+    const float zr = Z / R;
+    const float c = fmaxf(0.f, fminf(1.f, fabsf(zr / ell)));
+    const float d = c - ell;
+    const float vy = (sx * yw - sy * xw) / R / R, vx = (sx * xw + sy * yw) / R / R;
+    const float dc = d / c;
+    const float q = (1.f - dc * dc) / (1.f + dc * dc);
+    switch (preset) {
+        case 1: return 1.f / (c * c * (c * c + d * d));
+        case 2: return -2.f * q * q * (-vy) * (1.f + vx / zr) / (ell * ell) / R * R;
+        case 3: return 1.f / (zr * c * c);
+        case 4: return (vy / zr) / zr;
+        case 6: return -2.f * q * q / (1.f - dc) * (-vy) * (1.f + vx / zr) / zr;
+        default: return 1.f;  // preset 5 carries no extra factor
+    }
 }
 
 // (Z/L)^pL (Z/val)^pV, the direct-raycast weights (CB_backproject.cu:512-528).
@@ -260,7 +283,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     }
 
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
-    const bool needZ = P.pL != 0 || P.pV != 0;
+    const bool needZ = P.pL != 0 || P.pV != 0 || (RAYCAST && P.preset != 0);
     const int n_sub = P.ssx * P.ssy * P.ssz;
     for (int isub = 0; isub < n_sub; ++isub) {
         const int si = isub / (P.ssy * P.ssz), sj = (isub / P.ssz) % P.ssy, sk = isub % P.ssz;
@@ -296,9 +319,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         const float fv = fmaf(kf, (a2 == 0 ? bq.nv.x : (a2 == 1 ? bq.nv.y : bq.nv.z)) * vw,
                                               dot4(bq.nv, X, Y, Z)) * rD;
                         float w = RAYCAST ? 1.f : bq.kfast * rD * rD;
-                        if (needZ)
-                            w *= zpow(P, bq, fmaf(kf, (a2 == 0 ? bq.zl.x : (a2 == 1 ? bq.zl.y : bq.zl.z)) * vw,
-                                                  dot4(bq.zl, X, Y, Z)));
+                        if (needZ) {
+                            const float Zk = fmaf(kf, (a2 == 0 ? bq.zl.x : (a2 == 1 ? bq.zl.y : bq.zl.z)) * vw,
+                                                  dot4(bq.zl, X, Y, Z));
+                            w *= zpow(P, bq, Zk);
+                            if (RAYCAST && P.preset != 0)
+                                w *= preset_weight(P.preset, P.val, X + (a2 == 0 ? kf * vw : 0.f) + P.c0[0],
+                                                   Y + P.c0[1], bq.sxw, bq.syw, Zk);
+                        }
                         float pv;
                         if (BILIN) {
                             pv = fetch_bilinear(P, pvq, fu, fv);
@@ -467,7 +495,13 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                 const float fu = fmaf(kf, dNu, Nu0) * rD;
                                 const float fv = fmaf(kf, dNv, Nv0) * rD;
                                 float w = RAYCAST ? 1.f : b.kfast * rD * rD;
-                                if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
+                                if (needZ) {
+                                    const float Zk = fmaf(kf, dZ, Zb);
+                                    w *= zpow(P, b, Zk);
+                                    if (RAYCAST && P.preset != 0)
+                                        w *= preset_weight(P.preset, P.val, X0 + (a2 == 0 ? kf * vw : 0.f) + P.c0[0],
+                                                           Y0 + P.c0[1], b.sxw, b.syw, Zk);
+                                }
                                 // inner: inside the taper's flat box, which lies inside the
                                 // detector (|f - c| <= n/2 without a taper)
                                 const bool inner = fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv;
@@ -555,8 +589,9 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     if (cfg->apply_summand_multiplier != (multiplier_dev != nullptr ? 1u : 0u))
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
                        "apply_summand_multiplier must be set if and only if a multiplier is given");
-    if (cfg->weighting_preset != 0)
-        return ab_fail(APRICT_ERR_UNSUPPORTED, "backprojection weighting preset %u is not implemented",
+    if (cfg->weighting_preset > 6)
+        return ab_fail(APRICT_ERR_UNSUPPORTED,
+                       "backprojection weighting preset %u (the GBC formula) is not implemented",
                        cfg->weighting_preset);
     if (cfg->ssx == 0 || cfg->ssy == 0 || cfg->ssz == 0 || cfg->ssx > 16 || cfg->ssy > 16 || cfg->ssz > 16)
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ssx/ssy/ssz must be in [1, 16]");
@@ -613,6 +648,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.pV = cfg->Z_on_val_factor_power;
     P.val = cfg->Z_on_val_factor_val;
     P.inv_val = P.val != 0.f ? (float)(1.0 / (double)P.val) : 0.f;
+    P.preset = (int)cfg->weighting_preset;
     P.ssx = (int)cfg->ssx;
     P.ssy = (int)cfg->ssy;
     P.ssz = (int)cfg->ssz;

@@ -38,6 +38,7 @@ struct ab_bpview {
     // rounding is certain to pick the pixel the exact value picks (see
     // ab_fp32_pixel_error_bound); above it the choice is made in FP64.
     float tie_u, tie_v;
+    float sxw, syw;  // source position (world x, y), for the cone-cylinder weighting presets
 };
 
 // A priori bound on the error of the FP32 detector coordinate f = N(x)/D(x)
@@ -126,6 +127,8 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     const double ev = 1.5 * ab_fp32_pixel_error_bound(Av, ab_dot(Av, c0s), n, bdn, half_ext, fmax);
     o.tie_u = (float)(0.5 - (eu > 1e-4 ? eu : 1e-4));
     o.tie_v = (float)(0.5 - (ev > 1e-4 ? ev : 1e-4));
+    o.sxw = (float)s.x;
+    o.syw = (float)s.y;
     return true;
 }
 

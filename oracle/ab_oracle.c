@@ -15,7 +15,7 @@
  * ceil(c)-1 (reference :189-203, :244-246).
  *
  * The voxel-driven backprojector follows _backproject_CB_getval
- * (src/aprict/data/cusrc/CB_backproject.cu:313-733) for weighting preset 0.
+ * (src/aprict/data/cusrc/CB_backproject.cu:313-733) for weighting presets 0-6.
  */
 #include "ab_oracle.h"
 
@@ -259,6 +259,28 @@ static d3 voxel_centre(const ao_grid *g, int ix, int iy, int iz) {
                 g->corner[2] + (iz + 0.5) * g->voxwid};
 }
 
+/* Cone-cylinder weighting presets of the direct-raycast mode
+ * (CB_backproject.cu:530-599), R = config val; x the voxel, s the source,
+ * Z = (x - s).L / |L|. */
+static double preset_weight(int preset, double R, d3 x, d3 s, double Z) {
+    const d3 rs = sub(x, s);
+    const double ell = sqrt(rs.x * rs.x + rs.y * rs.y) / R;
+    const double zr = Z / R;
+    const double c = fmax(0.0, fmin(1.0, fabs(zr / ell)));
+    const double d = c - ell;
+    const double vy = (s.x * x.y - s.y * x.x) / R / R, vx = (s.x * x.x + s.y * x.y) / R / R;
+    const double dc = d / c;
+    const double q = (1.0 - dc * dc) / (1.0 + dc * dc);
+    switch (preset) {
+        case 1: return 1.0 / (c * c * (c * c + d * d));
+        case 2: return -2.0 * q * q * (-vy) * (1.0 + vx / zr) / (ell * ell) / R * R;
+        case 3: return 1.0 / (zr * c * c);
+        case 4: return (vy / zr) / zr;
+        case 6: return -2.0 * q * q / (1.0 - dc) * (-vy) * (1.0 + vx / zr) / zr;
+        default: return 1.0; /* preset 5 carries no extra factor */
+    }
+}
+
 /* Value one (sub-)voxel at x receives from view m in fast mode. */
 static double fast_value(const ao_proj_spec *sp, const double *img, d3 x, double voxwid, const ao_bp_cfg *c) {
     const d3 s = d3f(sp->source_pos), P = d3f(sp->det_pos), U = d3f(sp->det_u), V = d3f(sp->det_v);
@@ -287,6 +309,7 @@ static double fast_value(const ao_proj_spec *sp, const double *img, d3 x, double
         const double Z = dot(sub(x, s), L) / nrm(L);
         if (c->pL) mult *= powint(Z / nrm(L), c->pL);
         if (c->pV) mult *= powint(Z / c->val, c->pV);
+        if (c->preset >= 1 && c->preset <= 6) mult *= preset_weight(c->preset, c->val, x, s, Z);
         value = pv * mult;
     } else {
         const d3 detp = add(P, add(scl(U, cu), scl(V, cv)));

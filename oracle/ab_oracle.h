@@ -31,6 +31,7 @@ typedef struct {
     double val;
     int raycast, linear;
     int ssx, ssy, ssz;
+    int preset; /* direct-raycast weighting preset 0-6 (CB_backproject.cu:530-599) */
 } ao_bp_cfg;
 
 /* out[m,iu,iv] += mba * line integrals (ssu x ssv sub-rays averaged),
@@ -45,7 +46,7 @@ void ao_backproject_transpose(const ao_proj_spec *specs, int n_views, int nu, in
                               int nthreads);
 
 /* vol += mult * BP(projs), the voxel-driven backprojector of
- * _backproject_CB_getval (CB_backproject.cu:313-733), preset 0, in FP64. */
+ * _backproject_CB_getval (CB_backproject.cu:313-733), presets 0-6, in FP64. */
 void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
                     const ao_grid *g, const double *mult, const ao_bp_cfg *cfg, double *vol, int nthreads);
 

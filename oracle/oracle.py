@@ -64,6 +64,7 @@ class AoBpCfg(ctypes.Structure):
         ("ssx", ctypes.c_int),
         ("ssy", ctypes.c_int),
         ("ssz", ctypes.c_int),
+        ("preset", ctypes.c_int),
     ]
 
 
@@ -203,6 +204,7 @@ def bp_cfg_from_contents(c: np.ndarray) -> AoBpCfg:
     k.val = float(c["Z_on_val_factor_val"])
     k.raycast = int(c["approx_mode_direct_raycast"])
     k.linear = int(c["approx_mode_linear_interpolate"])
+    k.preset = int(c["weighting_preset"])
     k.ssx, k.ssy, k.ssz = int(c["ssx"]), int(c["ssy"]), int(c["ssz"])
     return k
 
@@ -296,7 +298,7 @@ def ref_backproject(
         None if mm is None else _p(mm), int(c["exact"]), int(c["backproject_all_1s"]), int(c["mask_to_cylinder"]),
         f(float(c["mask_to_cyl_rad"])), f(float(c["soften_edge_proportion"])), int(c["Z_on_L_factor_power"]),
         int(c["Z_on_val_factor_power"]), f(float(c["Z_on_val_factor_val"])), int(c["approx_mode_direct_raycast"]),
-        int(c["approx_mode_linear_interpolate"]), int(c["ssx"]), int(c["ssy"]), int(c["ssz"]),
+        int(c["approx_mode_linear_interpolate"]), int(c["ssx"]), int(c["ssy"]), int(c["ssz"]), int(c["weighting_preset"]),
         nthreads or nthreads_default(),
     )
     if oob:

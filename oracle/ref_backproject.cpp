@@ -28,7 +28,7 @@ long long ref_backproject(const void *specs, unsigned n_views, unsigned nu, unsi
                           float *vol, unsigned nx, unsigned ny, unsigned nz, float voxwid, const float *texpos,
                           const float *mult, int exact, int all_ones, int mask, float mask_rad, float sep, int pL,
                           int pV, float val, int raycast, int linear, unsigned ssx, unsigned ssy, unsigned ssz,
-                          int nthreads) {
+                          int preset, int nthreads) {
     ab_surface surf{(unsigned char *)vol, nz, ny, nx, sizeof(float), 0};
     ab_surface msurf{(unsigned char *)mult, nz, ny, nx, sizeof(float), 0};
     refb::config_CB_backproject cfg{};
@@ -43,7 +43,7 @@ long long ref_backproject(const void *specs, unsigned n_views, unsigned nu, unsi
     cfg.Z_on_val_factor_val = val;
     cfg.approx_mode_direct_raycast = raycast != 0;
     cfg.approx_mode_linear_interpolate = linear != 0;
-    cfg.backproj_weighting_preset = 0;
+    cfg.backproj_weighting_preset = (unsigned char)preset;
     cfg.ssx = ssx;
     cfg.ssy = ssy;
     cfg.ssz = ssz;

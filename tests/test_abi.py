@@ -112,8 +112,8 @@ def test_backproject_validation() -> None:
     cfg = fp.ConfigBackproject(apply_summand_multiplier=True).contents
     rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
     assert rc == 1
-    # weighting presets other than 0 are not implemented
-    cfg = fp.ConfigBackproject(backproj_weighting_preset=3).contents
+    # weighting preset 7 (the GBC formula) is not implemented
+    cfg = fp.ConfigBackproject(backproj_weighting_preset=7).contents
     rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
     assert rc == 2
     with pytest.raises(NotImplementedError):

@@ -178,3 +178,29 @@ def test_single_slice_volumes(case: str) -> None:
     want = O.backproject(pg.to_proj_spec_array(), projs, shape, cfg.contents, voxwid=1.0, corner=corner)
     assert np.linalg.norm(want) > 0
     assert rel_l2(v.as_numpy(), want) <= TOL
+
+
+@pytest.mark.parametrize("preset", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("bilinear", [False, True])
+def test_cone_cylinder_weighting_presets(preset: int, bilinear: bool) -> None:
+    """Direct-raycast weighting presets 1-6 (CB_backproject.cu:530-599) against the
+    FP64 oracle and the reference's own kernel body (R = the source radius)."""
+    R = 120.0  # noqa: N806
+    cfg = fp.ConfigBackproject(fast_approx=True, approx_mode_direct_raycast=True, Z_on_val_factor_val=R,
+                               Z_on_val_factor_power=-1, backproj_weighting_preset=preset,
+                               approx_mode_bilinear_interpolate=bilinear)
+    pg = circular(12, R, 120, 0.537, 48, 52)
+    projs = _projs(pg, 7)
+    got = _gpu_bp(cfg, pg, projs, pos_c=(0.4, -0.3, 0.2))
+    want = _oracle_bp(cfg, pg, projs, pos_c=(0.4, -0.3, 0.2))
+    assert np.linalg.norm(want) > 0
+    assert rel_l2(got, want) <= TOL
+    if O.have_ref():
+        ref = np.zeros(SHAPE, np.float32)
+        corner = np.array((0.4, -0.3, 0.2), np.float32) - np.array(SHAPE, np.float32) / 2
+        O.ref_backproject(pg.to_proj_spec_array(), projs, ref, cfg.contents, voxwid=1.0, corner=corner)
+        if bilinear:
+            assert rel_l2(got, ref) <= 1e-4
+        else:  # nearest: the reference's FP32 pixel choice flips at near-ties
+            flip = np.abs(got - ref) > 1e-4 * np.abs(want).max()
+            assert flip.mean() <= 1e-3
