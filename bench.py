@@ -178,16 +178,16 @@ def count_segments(pg, x_shape, voxwid: float, sample_views: int = 4) -> tuple[f
 
 def run_ours(args) -> dict:
     import torch
-    import torch.distributed as dist
 
     from aprict_b200 import Volume
     from aprict_b200.cb import flatpanel as fp
     from aprict_b200.iterators import SIRT_flatpanel
 
+    from aprict_b200 import replicas
+
     rank, world, local = _env_rank()
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    replicas.init("nccl")
     w = WORKLOADS[args.workload]
     n = w["n"]
     pg, x_true = make_problem(w)
@@ -198,17 +198,8 @@ def run_ours(args) -> dict:
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
 
-    def barrier() -> None:
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = replicas.barrier
+    max_over_ranks = replicas.max_over_ranks
 
     # ---- component kernels (CUDA events on the launching stream) ----
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -365,8 +356,7 @@ def run_ours(args) -> dict:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_reference(pg, x_true, w, b.cpu().numpy(), sirt)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
     return out if rank == 0 else {}
 
 
