@@ -23,7 +23,7 @@ from .volume import Volume
 KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V = 0, 1, 2, 3
 FP_TILE_V = (8, 16, 32)
 FP_WARP_V = (8, 16, 32)
-BP_XB = (2, 4)
+BP_XB = (2, 4, 8)
 BP_WAVE = (2, 3, 4, 6)
 
 _cache: dict[str, dict] = {}

@@ -9,8 +9,8 @@ namespace {
 using namespace ab_bp;
 
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
-__global__ void __launch_bounds__(kThreads, XB == 4 ? 2 : 3) k_backproject(const BPParams P) {
-    __shared__ BPSmem<EXACT, BILIN> sm;
+__global__ void __launch_bounds__(kThreads, bp_min_blocks(XB)) k_backproject(const BPParams P) {
+    __shared__ BPSmem<EXACT, BILIN, XB> sm;
     bp_brick<ORD, EXACT, RAYCAST, BILIN, XB>(P, blockIdx.x, sm);
 }
 
@@ -49,6 +49,11 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     const int ord = bp_ord(vd);
     if (ord == 2) {
         launch_bp<2, 2>(P, cfg, lin, (unsigned)grid, st);  // slices (xb forced to 2 below)
+    } else if (xb == 8) {
+        if (ord == 0)
+            launch_bp<0, 8>(P, cfg, lin, (unsigned)grid, st);
+        else
+            launch_bp<1, 8>(P, cfg, lin, (unsigned)grid, st);
     } else if (xb == 4) {
         if (ord == 0)
             launch_bp<0, 4>(P, cfg, lin, (unsigned)grid, st);

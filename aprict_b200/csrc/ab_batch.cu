@@ -136,12 +136,17 @@ __global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __gr
     retire(A.g);
 }
 
+// Voxels per thread of the batch backprojection kernel: the single-scan
+// default, two for slice stacks (as the single-scan launch).
+constexpr int batch_xb(int ord) { return ord == 2 ? 2 : ab_bp::kDefaultXB; }
+
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
-__global__ void __launch_bounds__(ab_bp::kThreads, 3) k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
-    __shared__ ab_bp::BPSmem<EXACT, BILIN> sm;
+__global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb(ORD)))
+    k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
+    __shared__ ab_bp::BPSmem<EXACT, BILIN, batch_xb(ORD)> sm;
     uint32_t unit;
     int s;
-    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, 2>(A.scans[s], unit, sm);
+    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD)>(A.scans[s], unit, sm);
     retire(A.g);
 }
 
@@ -276,11 +281,10 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             units[i] = u;
         } else {
             const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
-            int xb = 2;
+            int xb = 0;
             uint64_t u = 0;
-            // The batch kernel carries two voxels per thread.
             rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
-                                       cfg, sc.status_dev, bp[i], u, xb, 2);
+                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol)));
             if (rc != APRICT_OK) return scan_error(rc, i);
             const int v = bp_variant(cfg, &sc.vol);
             if (variant >= 0 && v != variant)

@@ -181,30 +181,42 @@ __device__ __forceinline__ float zpow(const BPParams &P, const ab_bpview &b, flo
 // RAYCAST: fast mode with direct-raycast weights (:512-646, preset 0).
 // BILIN: bilinear instead of nearest detector sampling.
 // ORD: 0 = C order (fastest axis z, slowest x), 1 = F order (fastest x).
-// XB: voxels per thread along the slowest axis (4: more reuse of each view's
-// coefficients, 2: fewer registers and more resident warps).
+// XB: voxels per thread along the slowest axis (2, 4 or 8: more reuse of each
+// view's coefficients against fewer registers per voxel).
 // Shared-memory staging of one chunk of per-view coefficients.
 // Fast modes also keep, per warp, a queue of deferred voxel-views (see
 // bp_brick) and the per-(lane, voxel) sums of their contributions.
 constexpr int kWarps = kThreads / 32;
-constexpr int kQCap = 32 + 32 * 4;  // a flush leaves < 32; one view adds <= 32 * XB
+// Queue entry: (view in chunk) << (5 + kbits) | k << 5 | lane, kbits = log2 XB.
+template <int XB>
+constexpr int q_kbits() { return XB == 2 ? 1 : (XB == 4 ? 2 : 3); }
+static_assert((kChunk - 1) << (5 + q_kbits<8>()) < 65536, "queue entries are 16 bits");
 
-template <bool EXACT, bool BILIN>
+// Resident CTAs per SM the kernels are compiled for (launch bounds), by XB;
+// also the default number of CTA waves per super-brick. The fast modes are
+// bound by the latency of the pixel gathers: more resident warps beat the few
+// registers spilled to (L1-resident) local memory at 64 registers a thread.
+constexpr int bp_min_blocks(int xb) { return xb == 8 ? 3 : 4; }
+constexpr int kDefaultXB = 4;
+
+template <bool EXACT, bool BILIN, int XB>
 struct BPSmem {
     static constexpr bool kNear = !EXACT && !BILIN;
+    static constexpr int kQCap = 32 + 32 * XB;  // a flush leaves < 32; one view adds <= 32 * XB
     ab_bpview sv[kChunk];
     ab_bpview_d svd[kNear ? kChunk : 1];
     ab_bpview_exact sx[EXACT ? kChunk : 1];
-    uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];   // (view in chunk) << 7 | k << 5 | lane
-    float qd[EXACT ? 1 : kWarps][EXACT ? 1 : 32 * 4];     // [lane * 4 + k]
+    uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];
+    float qd[EXACT ? 1 : kWarps][EXACT ? 1 : 32 * XB];  // [lane * XB + k]
 };
 
 // One backprojection work unit: brick `brick` (brick order) of the volume,
 // all views. Every thread of the CTA calls it with the same brick; it contains
 // __syncthreads and returns uniformly.
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
-__device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSmem<EXACT, BILIN> &sm) {
-    constexpr int kXB = XB;
+__device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSmem<EXACT, BILIN, XB> &sm) {
+    static_assert(XB == 2 || XB == 4 || XB == 8, "XB is 2, 4 or 8");
+    constexpr int kXB = XB, kKB = q_kbits<XB>();
     constexpr bool kNear = !EXACT && !BILIN;
     ab_bpview *sv = sm.sv;
     ab_bpview_d *svd = sm.svd;
@@ -266,6 +278,12 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     float acc[kXB];
 #pragma unroll
     for (int k = 0; k < kXB; ++k) acc[k] = 0.f;
+    // Nearest-pixel modes add each view's product one view late: the pixel
+    // loads of view t are still in flight while view t+1's coordinates are
+    // computed (the same additions in the same order as without the delay).
+    float pvp[kXB], wp[kXB];
+#pragma unroll
+    for (int k = 0; k < kXB; ++k) pvp[k] = wp[k] = 0.f;
 
     // Fast modes: voxel-views the branch-free pass cannot finish (near-tie
     // pixel choices, the detector-edge taper band; ~0.1-1 % of them) are not
@@ -279,7 +297,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     int qn = 0;
     if constexpr (!EXACT) {
 #pragma unroll
-        for (int k = 0; k < kXB; ++k) qd[lane * 4 + k] = 0.f;
+        for (int k = 0; k < kXB; ++k) qd[lane * kXB + k] = 0.f;
     }
 
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
@@ -298,7 +316,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                 auto flush = [&](int c, uint32_t v0) {
                     if (lane < c) {
                         const unsigned e = q[lane];
-                        const int L = (int)(e & 31u), k = (int)((e >> 5) & 3u), tt = (int)(e >> 7);
+                        const int L = (int)(e & 31u), k = (int)((e >> 5) & (kXB - 1u)), tt = (int)(e >> (5 + kKB));
                         // the owner's voxel (same formulas as its own pass)
                         int id[3];
                         id[a0] = b0 * 32 + L;
@@ -349,7 +367,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         }
                         float s = pv * w;
                         if (P.sep > 0.f && s != 0.f) s *= taper(bq, fu, fv, P.inv_sep);
-                        atomicAdd(&qd[L * 4 + k], s);
+                        atomicAdd(&qd[L * kXB + k], s);
                     }
                     __syncwarp();
                     const int rem = qn - c;
@@ -523,7 +541,13 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                     const int off = (__float_as_int(tu) - 0x4B400000) * P.su + (__float_as_int(tv) - 0x4B400000) * P.sv;
                                     if (live[k] && fast) pv = __ldg(pvw + off);
                                 }
-                                acc[k] = fmaf(pv, w, acc[k]);
+                                if (BILIN) {
+                                    acc[k] = fmaf(pv, w, acc[k]);
+                                } else {
+                                    acc[k] = fmaf(pvp[k], wp[k], acc[k]);
+                                    pvp[k] = pv;
+                                    wp[k] = w;
+                                }
                                 pending |= (live[k] && !fast) ? 1u << k : 0u;
                             }
                             if (__any_sync(0xffffffffu, pending != 0u)) {
@@ -531,7 +555,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                 for (int k = 0; k < kXB; ++k) {
                                     const bool p = (pending >> k) & 1u;
                                     const unsigned m = __ballot_sync(0xffffffffu, p);
-                                    if (p) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint16_t)((t << 7) | (k << 5) | lane);
+                                    if (p) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint16_t)((t << (5 + kKB)) | (k << 5) | lane);
                                     qn += __popc(m);
                                 }
                                 __syncwarp();
@@ -548,10 +572,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
         }
     }
 
+    if constexpr (!EXACT && !BILIN) {  // the last view's delayed products
+#pragma unroll
+        for (int k = 0; k < kXB; ++k) acc[k] = fmaf(pvp[k], wp[k], acc[k]);
+    }
     if constexpr (!EXACT) {  // the deferred contributions (all sub-samples)
         __syncwarp();
 #pragma unroll
-        for (int k = 0; k < kXB; ++k) acc[k] += qd[lane * 4 + k];
+        for (int k = 0; k < kXB; ++k) acc[k] += qd[lane * kXB + k];
     }
 
 #pragma unroll
@@ -576,7 +604,7 @@ inline int bp_ord(const aprict_vol_desc *vd) { return vd->order == 0 ? (vd->nz =
 
 // Host: validate one backprojection call and fill its parameters; units is
 // the number of work units (bricks, 0 when empty), xb the voxels per thread
-// (force_xb 2 or 4, or 0 for the tuning knob's choice).
+// (force_xb 2, 4 or 8, or 0 for the tuning knob's choice).
 inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd, const float *projs_dev,
                           const aprict_vol_desc *vd, float *vol_dev, const float *multiplier_dev,
                           const aprict_backproject_config *cfg, uint32_t *status_dev, BPParams &P,
@@ -654,7 +682,8 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.ssz = (int)cfg->ssz;
     P.status = status_dev;
 
-    xb = force_xb == 2 || force_xb == 4 ? force_xb : (ab_tuning_get(AB_TUNE_BP_XB) == 4 ? 4 : 2);
+    const int knob = ab_tuning_get(AB_TUNE_BP_XB);
+    xb = force_xb == 2 || force_xb == 4 || force_xb == 8 ? force_xb : (knob == 2 || knob == 8 ? knob : kDefaultXB);
     const int kXB = xb;
     const int ord = bp_ord(vd);
     if (ord == 2) {  // slices: lanes along y, warps x XB along x
@@ -676,7 +705,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
-    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : 3;
+    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : bp_min_blocks(xb);
     const double target = (double)wave * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
     int sb1 = (int)floor(sqrt(target * kXB / 8.0) + 0.5);
     sb1 = sb1 < 1 ? 1 : (sb1 > P.gb[1] ? P.gb[1] : sb1);

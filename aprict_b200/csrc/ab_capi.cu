@@ -101,7 +101,7 @@ int aprict_b200_set_tuning(int key, int value) {
     bool ok;
     switch (key) {
         case AB_TUNE_FP_TILE_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
-        case AB_TUNE_BP_XB: ok = value == 0 || value == 2 || value == 4; break;
+        case AB_TUNE_BP_XB: ok = value == 0 || value == 2 || value == 4 || value == 8; break;
         case AB_TUNE_FP_WARP_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
         default: ok = value >= 0 && value <= 16; break;
     }

@@ -133,7 +133,7 @@ def test_tuning_knobs_validate_and_round_trip() -> None:
     lib = _lib.lib()
     saved = [lib.aprict_b200_get_tuning(k) for k in range(4)]
     try:
-        for key, good, bad in [(0, (0, 8, 16, 32), (7, 64, -1)), (1, (0, 2, 4), (1, 3, 8)), (2, (0, 1, 16), (-1, 17)), (3, (0, 8, 16, 32), (4, 64))]:
+        for key, good, bad in [(0, (0, 8, 16, 32), (7, 64, -1)), (1, (0, 2, 4, 8), (1, 3, 16)), (2, (0, 1, 16), (-1, 17)), (3, (0, 8, 16, 32), (4, 64))]:
             for v in good:
                 assert lib.aprict_b200_set_tuning(key, v) == 0
                 assert lib.aprict_b200_get_tuning(key) == v
