@@ -9,7 +9,7 @@ namespace {
 using namespace ab_bp;
 
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
-__global__ void __launch_bounds__(kThreads, bp_min_blocks(XB)) k_backproject(const BPParams P) {
+__global__ void __launch_bounds__(kThreads, bp_min_blocks(XB, EXACT)) k_backproject(const BPParams P) {
     __shared__ BPSmem<EXACT, BILIN, XB> sm;
     bp_brick<ORD, EXACT, RAYCAST, BILIN, XB>(P, blockIdx.x, sm);
 }

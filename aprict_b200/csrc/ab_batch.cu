@@ -138,15 +138,15 @@ __global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __gr
 
 // Voxels per thread of the batch backprojection kernel: the single-scan
 // default, two for slice stacks (as the single-scan launch).
-constexpr int batch_xb(int ord) { return ord == 2 ? 2 : ab_bp::kDefaultXB; }
+constexpr int batch_xb(int ord, bool exact) { return ord == 2 ? 2 : ab_bp::default_xb(exact); }
 
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
-__global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb(ORD)))
+__global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb(ORD, EXACT), EXACT))
     k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
-    __shared__ ab_bp::BPSmem<EXACT, BILIN, batch_xb(ORD)> sm;
+    __shared__ ab_bp::BPSmem<EXACT, BILIN, batch_xb(ORD, EXACT)> sm;
     uint32_t unit;
     int s;
-    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD)>(A.scans[s], unit, sm);
+    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD, EXACT)>(A.scans[s], unit, sm);
     retire(A.g);
 }
 
@@ -284,7 +284,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             int xb = 0;
             uint64_t u = 0;
             rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
-                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol)));
+                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol), cfg->exact != 0));
             if (rc != APRICT_OK) return scan_error(rc, i);
             const int v = bp_variant(cfg, &sc.vol);
             if (variant >= 0 && v != variant)

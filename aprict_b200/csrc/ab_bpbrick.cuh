@@ -192,12 +192,16 @@ template <int XB>
 constexpr int q_kbits() { return XB == 2 ? 1 : (XB == 4 ? 2 : 3); }
 static_assert((kChunk - 1) << (5 + q_kbits<8>()) < 65536, "queue entries are 16 bits");
 
-// Resident CTAs per SM the kernels are compiled for (launch bounds), by XB;
-// also the default number of CTA waves per super-brick. The fast modes are
-// bound by the latency of the pixel gathers: more resident warps beat the few
-// registers spilled to (L1-resident) local memory at 64 registers a thread.
-constexpr int bp_min_blocks(int xb) { return xb == 8 ? 3 : 4; }
-constexpr int kDefaultXB = 4;
+// Resident CTAs per SM the kernels are compiled for (launch bounds), by XB
+// and mode; also the default number of CTA waves per super-brick. The fast
+// modes are bound by the latency of the pixel gathers: more resident warps
+// beat the few registers spilled to (L1-resident) local memory at 64
+// registers a thread, in the exact mode too.
+constexpr int kExactBlocks = 4;
+constexpr int bp_min_blocks(int xb, bool exact) { return exact ? kExactBlocks : (xb == 8 ? 3 : 4); }
+// Default voxels per thread: 4 in the fast modes, 2 in the exact mode (whose
+// per-voxel footprint loop gains nothing from sharing a view's coefficients).
+constexpr int default_xb(bool exact) { return exact ? 2 : 4; }
 
 template <bool EXACT, bool BILIN, int XB>
 struct BPSmem {
@@ -683,7 +687,8 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.status = status_dev;
 
     const int knob = ab_tuning_get(AB_TUNE_BP_XB);
-    xb = force_xb == 2 || force_xb == 4 || force_xb == 8 ? force_xb : (knob == 2 || knob == 8 ? knob : kDefaultXB);
+    xb = force_xb == 2 || force_xb == 4 || force_xb == 8 ? force_xb
+                                                       : (knob == 2 || knob == 4 || knob == 8 ? knob : default_xb(cfg->exact != 0));
     const int kXB = xb;
     const int ord = bp_ord(vd);
     if (ord == 2) {  // slices: lanes along y, warps x XB along x
@@ -705,7 +710,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
         cudaGetDevice(&dev);
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
     }
-    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : bp_min_blocks(xb);
+    const int wave = ab_tuning_get(AB_TUNE_BP_WAVE) > 0 ? ab_tuning_get(AB_TUNE_BP_WAVE) : bp_min_blocks(xb, cfg->exact != 0);
     const double target = (double)wave * sms / (double)P.gb[0];  // blocks of the (middle x slowest) plane per wave
     int sb1 = (int)floor(sqrt(target * kXB / 8.0) + 0.5);
     sb1 = sb1 < 1 ? 1 : (sb1 > P.gb[1] ? P.gb[1] : sb1);

@@ -127,7 +127,7 @@ APRICT_API const char *aprict_b200_version(void);
 
 /* Launch-shape knobs, process-wide (0 = built-in default). Keys:
  *   0 forward-projector tile height in pixels: 8, 16 or 32;
- *   1 backprojector voxels per thread along the slowest axis: 2, 4 (default) or 8;
+ *   1 backprojector voxels per thread along the slowest axis: 2, 4 or 8 (default 4, 2 in the exact mode);
  *   2 backprojector brick-order wave size in CTAs per SM: 1..16;
  *   3 forward-projector warp patch height (lanes along v): 8, 16 or 32.
  * Set by the autotuner (aprict_b200/autotune.py); results never depend on them. */

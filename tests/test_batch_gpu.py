@@ -81,7 +81,7 @@ def test_batched_residual_and_repeat_runs() -> None:
                                 dict()])
 def test_batched_backprojection_matches_one_scan_calls(kw) -> None:
     saved = autotune.current()
-    autotune.apply({"bp_xb": 4})  # the batch kernel's voxels per thread
+    autotune.apply({"bp_xb": 0})  # the built-in voxels per thread, as the batch kernel's
     try:
         vols, pgs = _scans(3, 6)
         rng = np.random.default_rng(5)
