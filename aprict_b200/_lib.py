@@ -54,6 +54,13 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
             ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
         ],
     ),
+    "aprict_b200_rotate_projections": (
+        _c_int,
+        [
+            _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_double, ctypes.c_double,
+            ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _c_void_p, _c_void_p, _c_void_p,
+        ],
+    ),
     "aprict_b200_forbild_compile": (_c_int, [_c_void_p, ctypes.c_int64, _c_void_p]),
     "aprict_b200_forbild_sample": (
         _c_int,
@@ -122,9 +129,11 @@ def check(status: int, where: str) -> None:
     raise AprictError(status, where, detail)
 
 
-def ptr(a: np.ndarray) -> int:
-    """Host address of a numpy array (struct arguments are passed by pointer)."""
-    return a.ctypes.data
+def ptr(a: np.ndarray) -> ctypes.c_void_p:
+    """Pointer to a numpy array's data (struct arguments are passed by
+    pointer). The pointer object holds a reference to the array, so a
+    temporary array stays alive for the duration of the call it is passed to."""
+    return a.ctypes.data_as(ctypes.c_void_p)
 
 
 def vol_desc(shape: tuple[int, int, int], order: str, voxwid: float, corner: np.ndarray) -> np.ndarray:

@@ -8,15 +8,18 @@ convolution, evaluated here directly by ``aprict_b200_ramp_filter`` (a
 shared-memory convolution kernel), one launch for the whole projection stack
 with the weights fused into the staging of each row.
 
-Scope: the fan-beam and FDK modes (``_hacky_fan_beam_mode`` /
-``_hacky_fdk_mode``), i.e. rotation angle 0. The cone-cylinder path that
-rotates each projection before filtering (:577-886) is not implemented and
-raises NotImplementedError.
+``FBPFilterer`` also filters along tilted lines for the cone-cylinder FBP
+(:577-886): each projection is padded to a wider frame, rotated by a random
+(or forced) angle, weighted, letterboxed, ramp-filtered along u and rotated
+back. Here the padding, rotation, weights and letterbox of a stack are one
+``aprict_b200_rotate_projections`` launch, the filter one convolution launch
+per kernel, and the back-rotation and crop one more launch per kernel.
 """
 
 from __future__ import annotations
 
 import enum
+import math
 import typing
 
 import numpy as np
@@ -113,13 +116,38 @@ class RampFilterer:
         return outs
 
 
+def frame_weight_mask(frame_shape: tuple[int, int], physpixwid: float, L: float, fdk: bool) -> np.ndarray:  # noqa: N803
+    """FP64 weights over the padded frame, computed from the reference's float32
+    pixel grids (ramp_filter.py:407-449): 1 / sqrt(1 + u^2 + v^2) for FDK,
+    otherwise 1 / ((1 + v^2)^(3/2) sqrt(1 + u^2 + v^2)), u and v in units of L."""
+    nu_e, nv_e = int(frame_shape[0]), int(frame_shape[1])
+    uarr = physpixwid / L * (np.arange(nu_e, dtype=np.float32) - (nu_e - 1) / 2)
+    varr = physpixwid / L * (np.arange(nv_e, dtype=np.float32) - (nv_e - 1) / 2)
+    if fdk:
+        mask = 1 / np.sqrt(1 + np.square(varr[np.newaxis, :]) + np.square(uarr[:, np.newaxis]))
+    else:
+        mask = 1 / (np.float_power(np.sqrt(1 + np.square(varr[np.newaxis, :])), 3)
+                    * np.sqrt(1 + np.square(varr[np.newaxis, :]) + np.square(uarr[:, np.newaxis])))
+    return np.ascontiguousarray(mask, dtype=np.float64)
+
+
 class FBPFilterer:
-    """Cosine-weighted ramp (and optionally Hilbert) filtering for FBP (ramp_filter.py:333-940)."""
+    """Weighted ramp (and optionally Hilbert) filtering for FBP (ramp_filter.py:333-886).
+
+    Fan-beam and FDK modes (``_hacky_fan_beam_mode`` / ``_hacky_fdk_mode``)
+    at rotation angle 0 fold the weights into the convolution's staging.
+    Otherwise each projection is filtered along lines tilted by its rotation
+    angle (random uniform in [-zeta, zeta], one ``rng.random()`` per
+    projection, or ``force_rotation_angle``).
+    """
 
     class SamplingStrategy(enum.Enum):
-        """Rotation sampling strategies of the reference (only angle 0 is implemented)."""
+        """Rotation sampling strategies of the reference."""
 
         SINGLE_ROTATION_RANDOM_UNIFORM = 1
+
+    # scratch budget of the tilted path per sub-chunk of views
+    _SCRATCH_BYTES = 512 << 20
 
     def __init__(
         self,
@@ -145,21 +173,30 @@ class FBPFilterer:
         self.hacky_fan_beam_mode = _hacky_fan_beam_mode
         self.hacky_fdk_mode = _hacky_fdk_mode
         self.ss = sampling_strategy
-        self.rng = np.random.default_rng() if rng is None else rng
+        self.projs_per_batch = int(projs_per_batch)
+        self.rng = np.random.default_rng(seed=None) if rng is None else rng
+        self._include_hilbert_transform = include_hilbert_transform_in_output
         self._max_abs_rotation_angle = self.get_max_abs_rotation_angle(self.proj_2d_shape, physpixwid, L)
         if limit_zeta is not None:
             self._max_abs_rotation_angle = min(self._max_abs_rotation_angle, limit_zeta)
+        self._expanded_2d_shape = self.get_expanded_proj_2d_shape(
+            self.proj_2d_shape, self._max_abs_rotation_angle, _hacky_fan_beam_mode, _hacky_fdk_mode
+        )
+        self.chunk_shape = (self.projs_per_batch, *self._expanded_2d_shape)
         funcs: tuple[KernFunc, ...] = (ramp_kernels.ramp_kernel_ramlak,)
         if include_hilbert_transform_in_output:
             funcs += (ramp_kernels.hilbert_transform_kernel,)
         # taps use the pixel pitch projected to distance 1 from the source (:393-395)
         self.rfilt = RampFilterer(
             physpixwid=physpixwid / L,
-            proj_2d_shape=self.proj_2d_shape,
+            proj_2d_shape=self._expanded_2d_shape,
             projs_per_batch=projs_per_batch,
             override_kern_funcs=funcs,
             apodization=apodization,
         )
+        self._mask_host = frame_weight_mask(self._expanded_2d_shape, physpixwid, L, _hacky_fdk_mode)
+        self._mask = torch.from_numpy(self._mask_host).cuda()
+        # Angle-0 fan/FDK path: the same weights folded into the convolution (FP32).
         nu, nv = self.proj_2d_shape
         u = physpixwid / L * (np.arange(nu, dtype=np.float64) - (nu - 1) / 2)
         v = physpixwid / L * (np.arange(nv, dtype=np.float64) - (nv - 1) / 2)
@@ -171,9 +208,50 @@ class FBPFilterer:
         self._weights_host = w
         self._weights = torch.from_numpy(w.astype(np.float32)).cuda()
 
+    # ---- the reference's helpers (ramp_filter.py:439-562) ----
+
+    def advance_rng(self, amount: int) -> None:
+        """Advance the internal rng by ``amount`` draws (as if that many projections were filtered)."""
+        for _ in range(amount):
+            self.rng.random()
+
+    def uniform_rng(self, low: float, high: float, len: int) -> np.ndarray:  # noqa: A002
+        """``len`` angles ``low + (high - low) * rng.random()`` as float32, one draw each (:443-460)."""
+        out = np.empty((len,), dtype=np.float32)
+        for i in range(len):
+            out[i] = low + (high - low) * self.rng.random()
+        return out
+
+    def get_letterbox_slice(self, rotation_angle: float) -> slice:
+        """Fractional column range of the rotated detector's vertical extent (:462-492)."""
+        if abs(rotation_angle) > self._max_abs_rotation_angle:
+            msg = "Invalid rotation angle entered."
+            raise ValueError(msg)
+        mid_index = (self._expanded_2d_shape[1] - 1) / 2
+        disc = self.L / self.physpixwid * np.sqrt(
+            np.maximum(np.square(np.cos(rotation_angle) / np.cos(self._max_abs_rotation_angle)) - 1, 0)
+        )
+        return slice(mid_index - disc, mid_index + disc)
+
+    def _letterbox_columns(self, rotation_angle: float) -> np.ndarray:
+        """Per-column factors of the letterbox multiplies (:690-749)."""
+        sl = self.get_letterbox_slice(rotation_angle)
+        w = np.ones(self._expanded_2d_shape[1])
+        i1, i2 = round(sl.start), round(sl.stop)
+        if i1 == i2:
+            w[i1] = sl.stop - sl.start
+            w[:i1] = 0
+            w[i1 + 1 :] = 0
+        else:
+            w[i1] = (i1 + 1 / 2) - sl.start
+            w[i2] = sl.stop - (i2 - 1 / 2)
+            w[:i1] = 0
+            w[i2 + 1 :] = 0
+        return w
+
     @property
     def zeta(self) -> float:
-        """Largest rotation angle the reference's rotated filtering would accept."""
+        """The largest rotation angle this object accommodates."""
         return self._max_abs_rotation_angle
 
     @classmethod
@@ -182,36 +260,128 @@ class FBPFilterer:
         nu, nv = int(proj_2d_shape[0]), int(proj_2d_shape[1])
         return float(np.arctan2(nv * physpixwid / 2, np.sqrt(L**2 + (nu * physpixwid / 2) ** 2)))
 
+    @classmethod
+    def get_expanded_proj_2d_shape(
+        cls,
+        proj_2d_shape: tuple[int, int],
+        max_abs_rotation_angle: float,
+        _hacky_fan_beam_mode: bool = False,
+        _hacky_fdk_mode: bool = False,
+    ) -> tuple[int, int]:
+        """The padded frame that holds every rotated projection (:516-562)."""
+        if _hacky_fan_beam_mode and _hacky_fdk_mode:
+            msg = "Cannot use both _hacky_fan_beam_mode and _hacky_fdk_mode."
+            raise ValueError(msg)
+        nu, nv = int(proj_2d_shape[0]), int(proj_2d_shape[1])
+        if _hacky_fan_beam_mode or _hacky_fdk_mode:
+            return nu, nv
+        s, c = np.sin(max_abs_rotation_angle), np.cos(max_abs_rotation_angle)
+        w, h = int(np.ceil(nv * s + nu * c)), int(np.ceil(nv))
+        return w + (w - nu) % 2, h + (h - nv) % 2
+
     @property
     def weights(self) -> np.ndarray:
-        """The (nu, nv) cosine weights (float64)."""
+        """The (nu, nv) weights of the angle-0 fan/FDK path (float64)."""
         return self._weights_host.copy()
+
+    @property
+    def mask(self) -> np.ndarray:
+        """The weight mask over the padded frame (float64)."""
+        return self._mask_host.copy()
+
+    # ---- filtering ----
+
+    def _angles(self, n: int, force_rotation_angle: float | None) -> np.ndarray:
+        if force_rotation_angle is None:
+            return self.uniform_rng(-self._max_abs_rotation_angle, self._max_abs_rotation_angle, n)
+        return force_rotation_angle * np.ones((n,), dtype=np.float32)
+
+    @staticmethod
+    def _cs(angles_deg: np.ndarray) -> np.ndarray:
+        # the library's chain: numpy.deg2rad in the angles' dtype, then math.cos / math.sin
+        rad = np.deg2rad(angles_deg)
+        return np.array([[math.cos(r), math.sin(r)] for r in rad], dtype=np.float64)
+
+    def _filter_tilted(self, data: torch.Tensor, angles: np.ndarray, outs: list[torch.Tensor]) -> None:
+        """Filter (n, nu, nv) ``data`` along lines tilted by ``angles`` into ``outs``."""
+        n = data.shape[0]
+        nu_e, nv_e = self._expanded_2d_shape
+        nu, nv = self.proj_2d_shape
+        padx, pady = (nu_e - nu) // 2, (nv_e - nv) // 2
+        cu, cv = (nu_e - 1) / 2, (nv_e - 1) / 2
+        hacky = self.hacky_fan_beam_mode or self.hacky_fdk_mode
+        per = max(1, min(n, self._SCRATCH_BYTES // (4 * nu_e * nv_e * (1 + self.rfilt.num_kerns))))
+        lib = _lib.lib()
+        for a in range(0, n, per):
+            b = min(n, a + per)
+            ang = angles[a:b]
+            cs_fwd = torch.from_numpy(self._cs(-180 / np.pi * ang)).cuda()
+            cs_bwd = torch.from_numpy(self._cs(180 / np.pi * ang)).cuda()
+            colw = None
+            if not hacky:
+                colw = torch.from_numpy(np.stack([self._letterbox_columns(x) for x in ang])).cuda()
+            frame = torch.empty((b - a, nu_e, nv_e), dtype=torch.float32, device=data.device)
+            src = data[a:b]
+            d_src, d_frame = _desc(src), _desc(frame)  # kept alive across the calls
+            _lib.check(
+                lib.aprict_b200_rotate_projections(
+                    _lib.ptr(d_src), src.data_ptr(), _lib.ptr(d_frame), frame.data_ptr(), cs_fwd.data_ptr(),
+                    cu, cv, padx, pady, 0, 0, self._mask.data_ptr(), None if colw is None else colw.data_ptr(),
+                    _stream(),
+                ),
+                "rotate_projections",
+            )
+            filtered = self.rfilt.filter(frame)
+            for f, out in zip(filtered, outs):
+                dst = out[a:b]
+                d_f, d_dst = _desc(f), _desc(dst)
+                _lib.check(
+                    lib.aprict_b200_rotate_projections(
+                        _lib.ptr(d_f), f.data_ptr(), _lib.ptr(d_dst), dst.data_ptr(), cs_bwd.data_ptr(),
+                        cu, cv, 0, 0, padx, pady, None, None, _stream(),
+                    ),
+                    "rotate_projections",
+                )
 
     def filter_bulk_axis1_concat(
         self,
         arr: torch.Tensor | np.ndarray,
-        block: bool = True,
-        clear_gpu_cache_regularly: bool = False,  # noqa: ARG002
+        clear_gpu_cache_regularly: bool = True,  # noqa: ARG002
         force_rotation_angle: float | None = None,
+        block: bool = True,
     ) -> tuple[list[torch.Tensor], torch.cuda.Event]:
-        """Weight and filter a whole (M, nu, nv) stack; returns (filtered arrays, completion event)."""
-        if not (self.hacky_fan_beam_mode or self.hacky_fdk_mode) or (force_rotation_angle not in (None, 0, 0.0)):
-            msg = "Only the fan-beam and FDK filtering modes (rotation angle 0) are implemented."
-            raise NotImplementedError(msg)
-        data = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).cuda() if isinstance(arr, np.ndarray) else arr
-        if tuple(data.shape[1:]) != self.proj_2d_shape:
+        """Filter a whole (M, nu, nv) stack; returns (one (M, nu, nv) array per filter, completion event)."""
+        if tuple(arr.shape[1:]) != self.proj_2d_shape:
             msg = "Wrong input size."
             raise ValueError(msg)
-        outs = self.rfilt.filter(data, weights=self._weights)
+        if isinstance(arr, np.ndarray):
+            data = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).cuda()
+        else:
+            data = arr
+            if data.dtype != torch.float32 or not data.is_cuda:
+                msg = "arr must be a float32 CUDA tensor or a host array"
+                raise ValueError(msg)
+        n = data.shape[0]
+        angles = self._angles(n, force_rotation_angle)
+        hacky = self.hacky_fan_beam_mode or self.hacky_fdk_mode
+        if hacky and not np.any(angles):
+            outs = self.rfilt.filter(data, weights=self._weights)  # padded frame == detector: no resampling
+        else:
+            outs = [torch.empty((n, *self.proj_2d_shape), dtype=torch.float32, device=data.device)
+                    for _ in range(self.rfilt.num_kerns)]
+            self._filter_tilted(data, angles, outs)
         ev = torch.cuda.Event()
         ev.record()
         if block:
             ev.synchronize()
         return outs, ev
 
-    def filter_bulk_axis1_stream(self, arr: torch.Tensor | np.ndarray, block: bool = True, **kw: object):  # noqa: ANN201
+    def filter_bulk_axis1_stream(self, arr: torch.Tensor | np.ndarray, block: bool = True, clear_gpu_cache_regularly: bool = False,
+                                 force_rotation_angle: float | None = None):  # noqa: ANN201
         """Generator form: yields (filtered arrays, event) per chunk of projs_per_batch projections."""
-        n = arr.shape[0]
-        per = self.rfilt.chunk_shape[0]
-        for i in range(0, n, per):
-            yield self.filter_bulk_axis1_concat(arr[i : i + per], block=block, **kw)
+        if tuple(arr.shape[1:]) != self.proj_2d_shape:
+            msg = "Wrong input size."
+            raise ValueError(msg)
+        for i in range(0, arr.shape[0], self.projs_per_batch):
+            yield self.filter_bulk_axis1_concat(arr[i : i + self.projs_per_batch], clear_gpu_cache_regularly,
+                                                force_rotation_angle, block)

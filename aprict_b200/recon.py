@@ -11,6 +11,15 @@ CB_backproject.cu:512-528) inside the reconstructable cylinder, and scale by
 Here the whole stack is filtered in one kernel launch with the weights and the
 final scale folded in, then backprojected in one launch (the reference loops
 over chunks of projections with several array passes each).
+
+``fbp_cone_cyl`` is the cone-cylinder (helical) FBP of the same script
+without the fan/FDK switches (recon_cbfp_cyl_fbp.py:366-701, 1107-1238):
+tilted filtering (FBPFilterer with one random rotation angle per projection,
+or the sum over ``num_rot_angs`` evenly spaced angles), the 2 zeta /
+sin^2(zeta/2) normalisation, direct-raycast backprojection with weighting
+preset 0 and (Z/R)^-3 (one-sided) or presets 1 and 6 with (Z/R)^-1 on the
+ramp- and Hilbert-filtered data (two-sided), and the scale
+(zs_max - zs_min) / (16 pi^2 R^2 M).
 """
 
 from __future__ import annotations
@@ -123,3 +132,84 @@ def fbp_fan_circ_batch(
     views = [fp.ProjectionSet(p.proj_geom, data=filtered[i * m : (i + 1) * m]) for i, p in enumerate(projs)]
     ScanBatch(volumes, views).backproject(cfg)
     return volumes
+
+
+def fbp_cone_cyl(
+    projs: fp.ProjectionSet,
+    volume: Volume,
+    *,
+    two_sided: bool = False,
+    num_rot_angs: int | None = None,
+    limit_zeta: float | None = None,
+    seed_proj_rots: int | None = None,
+    interpolate: bool = False,
+    ssx: int = 1,
+    ssy: int = 1,
+    ssz: int = 1,
+    cyl_mask_rad: float | None = None,
+    num_projs_per_chunk: int = 64,
+) -> Volume:
+    """Add the cone-cylinder FBP reconstruction of ``projs`` (M, nu, nv) into ``volume``.
+
+    Projections are filtered and backprojected ``num_projs_per_chunk`` at a
+    time; a chunk whose sources lie entirely out of reach of the volume along
+    z is skipped (its rotation angles are still drawn), as in the reference
+    (recon_cbfp_cyl_fbp.py:565-607).
+    """
+    if projs.data is None:
+        msg = "You must provide projection data."
+        raise ValueError(msg)
+    if num_projs_per_chunk <= 0:
+        msg = "num_projs_per_chunk must be positive"
+        raise ValueError(msg)
+    pg = projs.proj_geom
+    R, L, pixwid, nu, nv = fan_geometry(pg)  # noqa: N806
+    m = pg.num_projs
+    src_z = np.broadcast_to(pg.source_pos, pg.projs_list_shape + (3,))[:, 2].astype(np.float64)
+    zs_max, zs_min = float(src_z.max()), float(src_z.min())
+    vartheta_v = np.arctan2(nv * pixwid / 2 - pixwid / 2, np.sqrt(np.square(L) + np.square(nu * pixwid / 2 - pixwid / 2)))
+    support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
+    cyl_mask_rad = cyl_mask_rad or support
+    (x0, y0, z0), (x1, y1, z1) = volume.minxyz_maxxyz
+    max_r = min(cyl_mask_rad, float(np.sqrt(max(abs(x0), abs(x1)) ** 2 + max(abs(y0), abs(y1)) ** 2)))
+    vartheta_eff = min(limit_zeta, vartheta_v) if limit_zeta is not None else vartheta_v
+    hdiff = np.tan(vartheta_eff) * (R + max_r)
+    filt = FBPFilterer(
+        proj_2d_shape=(nu, nv), projs_per_batch=num_projs_per_chunk, L=L, physpixwid=pixwid, limit_zeta=limit_zeta,
+        include_hilbert_transform_in_output=two_sided, rng=np.random.default_rng(seed=seed_proj_rots),
+    )
+    zeta = filt.zeta
+    if num_rot_angs is None:
+        angs = None
+    elif num_rot_angs == 1:
+        angs = np.array([0.0], dtype=np.float32)
+    else:
+        angs = np.linspace(-zeta + (2 * zeta / num_rot_angs / 2), zeta - (2 * zeta / num_rot_angs / 2), endpoint=True,
+                           num=num_rot_angs)
+    norm = 2 * zeta / np.float_power(np.sin(zeta / 2), 2) / (1 if angs is None else len(angs))
+    scale = float(norm * (zs_max - zs_min) / (16 * np.square(np.pi) * R**2 * m))
+    common = dict(fast_approx=True, cyl_mask_rad=cyl_mask_rad, Z_on_val_factor_val=R, approx_mode_direct_raycast=True,
+                  approx_mode_bilinear_interpolate=interpolate, ssx=ssx, ssy=ssy, ssz=ssz)
+    if two_sided:
+        cfgs = [fp.ConfigBackproject(Z_on_val_factor_power=-1, backproj_weighting_preset=1, **common),
+                fp.ConfigBackproject(Z_on_val_factor_power=-1, backproj_weighting_preset=6, **common)]
+    else:
+        cfgs = [fp.ConfigBackproject(Z_on_val_factor_power=-3, backproj_weighting_preset=0, **common)]
+    data = projs.data
+    for a in range(0, m, num_projs_per_chunk):
+        sl = slice(a, min(m, a + num_projs_per_chunk))
+        if z1 < src_z[sl].min() - hdiff or z0 > src_z[sl].max() + hdiff:
+            filt.advance_rng(sl.stop - sl.start)  # out of reach of the volume
+            continue
+        chunk = data[sl]
+        if angs is None:
+            outs, _ = filt.filter_bulk_axis1_concat(chunk, force_rotation_angle=None, block=False)
+        else:
+            outs = None
+            for ang in angs:
+                o, _ = filt.filter_bulk_axis1_concat(chunk, force_rotation_angle=ang, block=False)
+                outs = o if outs is None else [x.add_(y) for x, y in zip(outs, o)]
+        for o, cfg in zip(outs, cfgs):
+            o.mul_(scale)
+            fp.backproject(cfg, volume, fp.ProjectionSet(pg.sliced(sl), data=o))
+    return volume

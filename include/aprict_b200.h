@@ -233,6 +233,27 @@ APRICT_API int aprict_b200_ramp_filter(const aprict_proj_desc *in, const float *
                                        int odd_taps_only, const float *weights_dev, int64_t w_stride_u,
                                        int64_t w_stride_v, float scale, aprict_stream_t stream);
 
+/* Rotated bilinear resampling of a projection stack: the per-projection
+ * rotations of the cone-cylinder FBP filter with its padding, weight mask,
+ * letterbox and crop (FBPFilterer.filter_bulk_axis1_stream,
+ * cb/ramp_filter.py:651-749 forward, :790-842 back; the rotations are
+ * cupyx.scipy.ndimage.rotate(order=1, mode="grid-constant", reshape=False,
+ * prefilter=False)). Both arrays live in one padded frame with rotation
+ * centre (centre_u, centre_v); in[0][0] sits at (in_off_u, in_off_v) and
+ * out[0][0] at (out_off_u, out_off_v). For view m and output pixel (i, j),
+ * with p = (i + out_off_u, j + out_off_v) - centre and (c, s) = cs_dev[2m],
+ * cs_dev[2m+1] (cosine and sine of the rotate() angle):
+ *   q   = (c p_u + s p_v, -s p_u + c p_v) + centre - (in_off_u, in_off_v)
+ *   x   = (float) bilinear(in[m], q)      FP64, neighbours outside in are 0
+ *   x   = (float)(x * mask_dev[i * nv_out + j])      if mask_dev (FP64)
+ *   out = (float)(x * colw_dev[m * nv_out + j])      if colw_dev (FP64)
+ * cs_dev, mask_dev and colw_dev are device arrays; in and out must not alias. */
+APRICT_API int aprict_b200_rotate_projections(const aprict_proj_desc *in, const float *in_dev,
+                                              const aprict_proj_desc *out, float *out_dev, const double *cs_dev,
+                                              double centre_u, double centre_v, int32_t in_off_u, int32_t in_off_v,
+                                              int32_t out_off_u, int32_t out_off_v, const double *mask_dev,
+                                              const double *colw_dev, aprict_stream_t stream);
+
 /* ---- Analytic (FORBILD) phantoms ---- */
 
 /* One clipping half-space (FORBILD_ClipAxisSpec, FORBILD_volumes.h:89-155):
