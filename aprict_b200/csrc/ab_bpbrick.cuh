@@ -37,6 +37,9 @@ struct BPParams {
     uint32_t n_views, nu, nv;
     int64_t stride_view;
     int su, sv;  // u, v element strides (in-view offsets are checked to fit 32 bits)
+    // -0x4B400000 (su + sv) mod 2^32: turns the bit patterns of two magic-rounded
+    // coordinates into the pixel offset with two multiply-adds
+    uint32_t koff;
     float fnu1, fnv1;  // nu + 1, nv + 1: clamp bounds for the rounded pixel index
     const float *projs;
     float *vol;
@@ -208,6 +211,7 @@ struct BPSmem {
     static constexpr bool kNear = !EXACT && !BILIN;
     static constexpr int kQCap = 32 + 32 * XB;  // a flush leaves < 32; one view adds <= 32 * XB
     ab_bpview sv[kChunk];
+    float4 sd[kChunk];  // per view: steps of N_u, N_v, D, Z along the thread's XB axis
     ab_bpview_d svd[kNear ? kChunk : 1];
     ab_bpview_exact sx[EXACT ? kChunk : 1];
     uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];
@@ -399,6 +403,11 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         if (!ab_derive_bpview(sp, c0d, vw, P.sep, hext, sv[t], kNear ? &svd[t] : nullptr) && P.status)
                             atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
+                        const ab_bpview &bt = sv[t];
+                        sm.sd[t] = make_float4((a2 == 0 ? bt.nu.x : (a2 == 1 ? bt.nu.y : bt.nu.z)) * vw,
+                                               (a2 == 0 ? bt.nv.x : (a2 == 1 ? bt.nv.y : bt.nv.z)) * vw,
+                                               (a2 == 0 ? bt.den.x : (a2 == 1 ? bt.den.y : bt.den.z)) * vw,
+                                               (a2 == 0 ? bt.zl.x : (a2 == 1 ? bt.zl.y : bt.zl.z)) * vw);
                     }
                     __syncthreads();
                     // warp-uniform skip (the fast modes' queue uses whole-warp votes)
@@ -409,13 +418,12 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         const float *pvw = P.projs + (int64_t)view * P.stride_view;
                         const float Nu0 = dot4(b.nu, X0, Y0, Z0), Nv0 = dot4(b.nv, X0, Y0, Z0);
                         const float D0 = dot4(b.den, X0, Y0, Z0);
-                        const float dNu = (a2 == 0 ? b.nu.x : (a2 == 1 ? b.nu.y : b.nu.z)) * vw;
-                        const float dNv = (a2 == 0 ? b.nv.x : (a2 == 1 ? b.nv.y : b.nv.z)) * vw;
-                        const float dD = (a2 == 0 ? b.den.x : (a2 == 1 ? b.den.y : b.den.z)) * vw;
+                        const float4 steps = sm.sd[t];
+                        const float dNu = steps.x, dNv = steps.y, dD = steps.z;
                         float Zb = 0.f, dZ = 0.f;
                         if (needZ) {
                             Zb = dot4(b.zl, X0, Y0, Z0);
-                            dZ = (a2 == 0 ? b.zl.x : (a2 == 1 ? b.zl.y : b.zl.z)) * vw;
+                            dZ = steps.w;
                         }
                         if constexpr (EXACT) {
 #pragma unroll
@@ -542,7 +550,10 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                     const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
                                     fast = inner && fabsf(du) <= b.tie_u && fabsf(dv) <= b.tie_v;
                                     // pixel offset from the rounded indices (bits - magic)
-                                    const int off = (__float_as_int(tu) - 0x4B400000) * P.su + (__float_as_int(tv) - 0x4B400000) * P.sv;
+                                    // (bits(tu) - 0x4B400000) su + (bits(tv) - 0x4B400000) sv, in
+                                    // wrapping unsigned arithmetic (the in-view offset fits 31 bits)
+                                    const int off = (int)((uint32_t)__float_as_int(tu) * (uint32_t)P.su +
+                                                          ((uint32_t)__float_as_int(tv) * (uint32_t)P.sv + P.koff));
                                     if (live[k] && fast) pv = __ldg(pvw + off);
                                 }
                                 if (BILIN) {
@@ -646,6 +657,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.stride_view = pd->stride_view;
     P.su = (int)pd->stride_u;
     P.sv = (int)pd->stride_v;
+    P.koff = 0u - 0x4B400000u * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
     P.fnu1 = (float)pd->nu + 1.f;
     P.fnv1 = (float)pd->nv + 1.f;
     P.projs = projs_dev;
