@@ -54,6 +54,25 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
             ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
         ],
     ),
+    "aprict_b200_vol_div_softzero": (
+        _c_int, [_c_void_p, _c_void_p, _c_void_p, ctypes.c_int64, ctypes.c_float, _c_void_p],
+    ),
+    "aprict_b200_vol_mul_xygrid": (_c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "aprict_b200_backproject_gbc": (
+        _c_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                 _c_void_p],
+    ),
+    "aprict_b200_gbc_weight_integral": (
+        _c_int, [_c_void_p, ctypes.c_int32, _c_void_p, ctypes.c_int32, ctypes.c_int32, _c_void_p, _c_void_p],
+    ),
+    "aprict_b200_conebeam_spectral": (
+        _c_int, [_c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                 ctypes.c_double, _c_void_p],
+    ),
+    "aprict_b200_add_upsampled": (
+        _c_int, [_c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _c_void_p, ctypes.c_int32, ctypes.c_int32,
+                 ctypes.c_int32, ctypes.c_int32, _c_void_p],
+    ),
     "aprict_b200_rotate_projections": (
         _c_int,
         [

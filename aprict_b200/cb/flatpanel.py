@@ -631,12 +631,34 @@ def backproject(
     if bool(cfg["apply_summand_multiplier"]) != (summand_multiplier is not None):
         msg = "To prevent unintended behaviour, the config 'apply_summand_multiplier' must be true if and only if a summand_multiplier is included."
         raise ValueError(msg)
-    if int(cfg["weighting_preset"]) > 6 or secondary_volume is not None:
-        msg = "Backprojection weighting preset 7 (the GBC formula, with its secondary volume) is not implemented."
+    preset = int(cfg["weighting_preset"])
+    if preset > 7:
+        msg = f"Backprojection weighting preset {preset} is not implemented."
         raise NotImplementedError(msg)
     _check_volume_device(volume)
     vd = volume._desc()  # noqa: SLF001
     mptr = summand_multiplier.data.data_ptr() if summand_multiplier is not None else None
+    if preset == 7:
+        # the GBC kernel, with the weight sums in the secondary volume (flatpanel.py:216-232)
+        if secondary_volume is None:
+            msg = "Weighting preset 7 (GBC) needs a secondary_volume to receive the sums of the weights."
+            raise ValueError(msg)
+        if secondary_volume.shape != volume.shape or secondary_volume.order != volume.order:
+            msg = "The secondary volume must have the volume's shape and memory order."
+            raise ValueError(msg)
+        _check_volume_device(secondary_volume)
+        for it, first in _leading_slices(projs):
+            specs, pd, dptr = _view_args(projs, it, first)
+            _lib.check(
+                _lib.lib().aprict_b200_backproject_gbc(
+                    specs, _lib.ptr(pd), dptr, _lib.ptr(vd), volume.data.data_ptr(), secondary_volume.data.data_ptr(),
+                    mptr, _lib.ptr(cfg), None, _stream(),
+                ),
+                "backproject_gbc",
+            )
+        if block:
+            torch.cuda.current_stream().synchronize()
+        return volume
     for it, first in _leading_slices(projs):
         specs, pd, dptr = _view_args(projs, it, first)
         _lib.check(

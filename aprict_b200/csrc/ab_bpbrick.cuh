@@ -634,7 +634,8 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
                        "apply_summand_multiplier must be set if and only if a multiplier is given");
     if (cfg->weighting_preset > 6)
         return ab_fail(APRICT_ERR_UNSUPPORTED,
-                       "backprojection weighting preset %u (the GBC formula) is not implemented",
+                       "backprojection weighting preset %u: presets 0-6 here, 7 (GBC) through "
+                       "aprict_b200_backproject_gbc",
                        cfg->weighting_preset);
     if (cfg->ssx == 0 || cfg->ssy == 0 || cfg->ssz == 0 || cfg->ssx > 16 || cfg->ssy > 16 || cfg->ssz > 16)
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ssx/ssy/ssz must be in [1, 16]");

@@ -1,0 +1,414 @@
+// ab_gbc.cu -- the GBC reconstruction's device work: backprojection with the
+// cylindrical-locus GBC weights into a volume and a weight-sum volume, the
+// expected weight sum over a perfect cylindrical trajectory, the volume-domain
+// cone-beam ramp filter's spectral multiplier, and the trilinear low-resolution
+// correction.
+//
+// Reference: backproject_CB_voltex_GBC_cyl / _backproject_CB_getval_GBC_cyl /
+// _GBC_weightfun / cossq_soft (src/aprict/data/cusrc/CB_backproject.cu:273-311,
+// 736-905, 1030-1105), get_GBC_weight_integ (:1108-1168, driven by
+// src/aprict/gbc/weightinteg.py:22-91), ramp_filter_conebeam and
+// _conebeam_kfactor_unchunked (src/aprict/gbc/filters.py:59-147, 256-504).
+//
+// The backprojection launches once for all views (the reference: once per 10
+// views, the volume read-modified-written each time). One thread per voxel,
+// consecutive threads on consecutive voxels in memory order, per-view
+// coefficients staged in shared memory. The weight is evaluated in FP32 with
+// the CUDA math library (atan2f, cosf, acosf, sinf), the detector coordinate
+// by the same linear forms as the other backprojection modes, and the
+// nearest-pixel choice re-decided in FP64 near ties, so the result follows
+// the FP64 restatement. The spectral filter is one pass over the cuFFT
+// spectrum with all per-frequency factors (ramp, 1 / k-factor, sinc
+// corrections, DC) folded into one FP64 factor; the reference makes about
+// ten array passes.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "ab_bpbrick.cuh"
+
+namespace {
+
+constexpr int kGThreads = 256;
+constexpr int kGChunk = 64;  // views per shared-memory chunk
+
+// Soft window s(a, b; c) of cossq_soft (CB_backproject.cu:273-311): 0 beyond
+// |c| = a, 1 inside |c| = a - b, 3x^2 - 2x^3 between, x = gamma sin|c| - chi.
+__device__ float cossq_soft(float a, float b, float c) {
+    if (fabsf(c) > a) return 0.f;
+    if (fabsf(c) < a - b) return 1.f;
+    const float gamma = 1.f / (sinf(a - b) - sinf(a));
+    const float chi = gamma * sinf(a);
+    const float x = gamma * sinf(fabsf(c)) - chi;
+    return fmaxf(0.f, fminf(1.f, 3.f * x * x - 2.f * x * x * x));
+}
+
+struct GbcSoft {
+    float v, v_span, h, h_span;  // soft_vartheta_v, its span, soft_vartheta_h, its span
+};
+
+// GBC weight (eq. 23 of the GBC method with the soft windows,
+// CB_backproject.cu:736-787) of the voxel at world position p for the source
+// at s, R the radius of the source cylinder about the world z axis.
+__device__ float gbc_weight(float R, float px, float py, float pz, float sx, float sy, float sz, const GbcSoft &S) {
+    const float lx = -sx, ly = -sy;  // L = (-s_x, -s_y, 0)
+    const float rx = px - sx, ry = py - sy, rz = pz - sz;
+    const float Z = (rx * lx + ry * ly) / sqrtf(lx * lx + ly * ly);
+    const float ell_on_R = sqrtf(rx * rx + ry * ry) / R;
+    const float Z_on_R = Z / R;
+    const float c_on_R = fmaxf(0.f, fminf(1.f, fabsf(Z_on_R / ell_on_R)));
+    const float d_on_R = c_on_R - ell_on_R;
+    const float theta_el = atan2f(rz / R, ell_on_R);
+    const float cos_el = cosf(theta_el);
+    const float weight = cos_el * cos_el * cos_el * c_on_R / fmaxf(1e-9f, c_on_R * c_on_R + d_on_R * d_on_R);
+    const float soft = cossq_soft(S.v, S.v_span, theta_el) * cossq_soft(S.h, S.h_span, acosf(c_on_R));
+    return weight * soft;
+}
+
+struct GbcParams {
+    float *vol2;  // weight-sum volume (same layout as the volume)
+    float R;
+    GbcSoft soft;
+    float pos000[3];  // world centre of voxel (0, 0, 0): corner + voxwid / 2
+};
+
+template <bool BILIN>
+__global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPParams P, const GbcParams G,
+                                                               int order_f) {
+    using namespace ab_bp;
+    __shared__ ab_bpview sv[kGChunk];
+    __shared__ ab_bpview_d svd[BILIN ? 1 : kGChunk];
+    __shared__ float ssrc[kGChunk][3];
+
+    const int64_t nvox = (int64_t)P.n[0] * P.n[1] * P.n[2];
+    const int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x;
+    const bool live = e < nvox;
+    int id[3];
+    if (order_f) {  // x fastest
+        id[0] = (int)(e % P.n[0]);
+        id[1] = (int)((e / P.n[0]) % P.n[1]);
+        id[2] = (int)(e / ((int64_t)P.n[0] * P.n[1]));
+    } else {  // z fastest
+        id[2] = (int)(e % P.n[2]);
+        id[1] = (int)((e / P.n[2]) % P.n[1]);
+        id[0] = (int)(e / ((int64_t)P.n[1] * P.n[2]));
+    }
+    const float vw = P.voxwid;
+    const float offs[3] = {1.f / (float)P.ssx, 1.f / (float)P.ssy, 1.f / (float)P.ssz};
+    const int n_sub = P.ssx * P.ssy * P.ssz;
+    float acc = 0.f, acc2 = 0.f;
+
+    for (uint32_t v0 = 0; v0 < P.n_views; v0 += kGChunk) {
+        const int cn = (int)min((uint32_t)kGChunk, P.n_views - v0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cn; t += kGThreads) {
+            const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
+                            P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
+            const aprict_proj_spec sp = P.specs[v0 + t];
+            const double hext[3] = {(0.5 * P.n[0] + 1.0) * P.vwd, (0.5 * P.n[1] + 1.0) * P.vwd,
+                                    (0.5 * P.n[2] + 1.0) * P.vwd};
+            if (!ab_derive_bpview(sp, c0d, vw, 0.f, hext, sv[t], BILIN ? nullptr : &svd[t]) && P.status)
+                atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
+            ssrc[t][0] = sp.source_pos.x;
+            ssrc[t][1] = sp.source_pos.y;
+            ssrc[t][2] = sp.source_pos.z;
+        }
+        __syncthreads();
+        if (!live) continue;
+        for (int isub = 0; isub < n_sub; ++isub) {
+            const int sidx[3] = {isub / (P.ssy * P.ssz), (isub / P.ssz) % P.ssy, isub % P.ssz};
+            float fsub[3], rel[3], wp[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                fsub[a] = -0.5f + offs[a] * (0.5f + (float)sidx[a]);
+                // relative to the volume centre, for the detector coordinate
+                rel[a] = ((float)id[a] + 0.5f - 0.5f * (float)P.n[a]) * vw + fsub[a] * vw;
+                // world position as the reference forms it (pos_000_c + idx voxwid + offset voxwid)
+                wp[a] = (G.pos000[a] + (float)id[a] * vw) + fsub[a] * vw;
+            }
+            float s = 0.f, s2 = 0.f;
+            for (int t = 0; t < cn; ++t) {
+                const float w = gbc_weight(G.R, wp[0], wp[1], wp[2], ssrc[t][0], ssrc[t][1], ssrc[t][2], G.soft);
+                s2 += w;
+                if (w == 0.f) continue;
+                const ab_bpview &b = sv[t];
+                const float rD = rcp_fast(dot4(b.den, rel[0], rel[1], rel[2]));
+                const float fu = dot4(b.nu, rel[0], rel[1], rel[2]) * rD;
+                const float fv = dot4(b.nv, rel[0], rel[1], rel[2]) * rD;
+                const float *pvw = P.projs + (int64_t)(v0 + t) * P.stride_view;
+                float pv;
+                if (BILIN) {
+                    pv = fetch_bilinear(P, pvw, fu, fv);
+                } else {
+                    float du, dv;
+                    int iu = round_index(fu, -2.f, P.fnu1, du);
+                    int iv = round_index(fv, -2.f, P.fnv1, dv);
+                    const bool tu = fabsf(du) > b.tie_u, tv = fabsf(dv) > b.tie_v;
+                    if (tu || tv) {
+                        const VoxRef vr{((double)id[0] + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                        ((double)id[1] + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                        ((double)id[2] + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) * P.vwd};
+                        const ab_bpview_d &cd = svd[BILIN ? 0 : t];
+                        if (tu) iu = refine_index(cd.nu, cd.den, vr, iu, du);
+                        if (tv) iv = refine_index(cd.nv, cd.den, vr, iv, dv);
+                    }
+                    const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
+                    pv = inb ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
+                }
+                s = fmaf(pv, w, s);
+            }
+            acc += s;
+            acc2 += s2;
+        }
+    }
+    if (!live) return;
+    const float value = n_sub == 1 ? acc : acc / (float)n_sub;
+    const float value2 = n_sub == 1 ? acc2 : acc2 / (float)n_sub;
+    if (value == 0.f && value2 == 0.f) return;  // the reference writes neither (:1068-1075)
+    const int64_t o = (int64_t)id[0] * P.vs[0] + (int64_t)id[1] * P.vs[1] + (int64_t)id[2] * P.vs[2];
+    const float m = P.mult ? P.mult[o] : 1.f;
+    if (value != 0.f) P.vol[o] = value * m + P.vol[o];
+    if (value2 != 0.f) G.vol2[o] = value2 * m + G.vol2[o];
+}
+
+// Expected GBC weight sum at radius r (units of R) over a perfect cylindrical
+// source locus: sum over num_z heights z in [0, tan(vartheta_v) (1 + r_max)]
+// (the first with weight 1/2) and num_ang source angles t in [0, pi) of the
+// weight of the voxel (r, 0, 0) for the source (cos t, sin t, z), times
+// 4 z_max pi / (num_z num_ang) (get_GBC_weight_integ, CB_backproject.cu:1108-1168).
+// One thread per (z, angle) sample; per radius an FP64 block sum and one
+// atomic add.
+__global__ void __launch_bounds__(kGThreads) k_gbc_weight_integ(const float *r_on_R, int nr, double *out, int num_z,
+                                                                int num_ang, GbcSoft S) {
+    __shared__ double warp_sums[kGThreads / 32];
+    const int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x;
+    const bool live = e < (int64_t)num_z * num_ang;
+    const int iz = live ? (int)(e / num_ang) : 0, ia = live ? (int)(e % num_ang) : 0;
+    const float maxz = tanf(S.v) * (1.f + r_on_R[nr - 1]);
+    const float z = maxz * (float)iz / (float)(num_z - 1);
+    const float t = (float)ia / (float)num_ang * 3.1415926535898f;
+    const float sx = cosf(t), sy = sinf(t);
+    const float half = iz == 0 ? 0.5f : 1.f;
+    const double mult = (double)((4.f * maxz * 3.1415926535898f) / ((float)num_z * (float)num_ang));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = 0; r < nr; ++r) {
+        double w = live ? (double)(gbc_weight(1.f, r_on_R[r], 0.f, 0.f, sx, sy, z, S) * half) : 0.0;
+#pragma unroll
+        for (int k = 16; k > 0; k >>= 1) w += __shfl_xor_sync(0xffffffffu, w, k);
+        if (lane == 0) warp_sums[warp] = w;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int k = 0; k < kGThreads / 32; ++k) b += warp_sums[k];
+            if (b != 0.0) atomicAdd(out + r, b * mult);
+        }
+        __syncthreads();
+    }
+}
+
+// k-factor of the softened Colsher window at polar angle th (radians from
+// the k_z axis, |th| taken), cone angle `cone` and softening `soft`
+// (_conebeam_kfactor_unchunked, gbc/filters.py:59-147): 2 pi outside
+// (cone/2 - soft, pi - (cone/2 - soft)), else the cubic in sin(th).
+__device__ double conebeam_kfactor(double th, double cone, double soft) {
+    th = fabs(th);
+    const double h = cone / 2 - soft;
+    if (!(h < th && th < M_PI - h)) return 2 * M_PI;
+    const double gamma = 1.0 / (sin(cone / 2 - soft) - sin(cone / 2));
+    const double chi = gamma * sin(cone / 2);
+    const double s = sin(th);
+    const double alpha = h <= 0 ? 0.0 : fmax(0.0, fmin(1.0, sin(h) / s));
+    const double beta = fmax(0.0, fmin(1.0, sin(cone / 2) >= s ? 1.0 : sin(cone / 2) / s));
+    const double t1 = asin(beta) - asin(alpha);
+    const double t2 = sqrt(1 - beta * beta);
+    const double t3 = sqrt(1 - alpha * alpha);
+    double out = t1 * 4 * (chi * chi) * (3 + 2 * chi) + 4 * asin(alpha);
+    out += s * (24 * gamma * chi * (1 + chi) * (t2 - t3));
+    out += s * s * (6 * gamma * gamma * (1 + 2 * chi) * (t1 - beta * t2 + alpha * t3));
+    out += s * s * s * (-2.0 / 3.0 * gamma * gamma * gamma * (-9 * (t2 - t3) + (cos(3 * asin(beta)) - cos(3 * asin(alpha)))));
+    return out;
+}
+
+__device__ double fftfreq(int k, int n) { return (double)(k < (n + 1) / 2 ? k : k - n) / (double)n; }
+
+__device__ double sinc(double x) {
+    if (x == 0.0) return 1.0;
+    const double px = M_PI * x;
+    return sin(px) / px;
+}
+
+struct SpecParams {
+    float2 *spec;  // (n0, n1, n2 / 2 + 1) complex, C order
+    int n0, n1, n2;
+    double multiplier, cone, soft;
+};
+
+// One pass over the rfftn spectrum of an (n0, n1, n2) volume (axis 2 = z,
+// the cylinder axis): times |k| * multiplier, divided by the k-factor of the
+// polar angle (cone > 0; cone = pi gives 2 pi; cone = 0 uses the lateral |k|
+// without a k-factor), times sinc(f0) sinc(f1) sinc(f2); the DC term is set
+// to 0 (filters.py:340-398).
+__global__ void __launch_bounds__(kGThreads) k_conebeam_spectral(const SpecParams P) {
+    const int m2 = P.n2 / 2 + 1;
+    const int64_t n = (int64_t)P.n0 * P.n1 * m2;
+    const int64_t step = (int64_t)gridDim.x * kGThreads;
+    for (int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x; e < n; e += step) {
+        const int k2 = (int)(e % m2);
+        const int64_t r = e / m2;
+        const int k1 = (int)(r % P.n1), k0 = (int)(r / P.n1);
+        const double f0 = fftfreq(k0, P.n0), f1 = fftfreq(k1, P.n1), f2 = (double)k2 / (double)P.n2;
+        const double lat2 = f0 * f0 + f1 * f1;
+        double factor;
+        if (P.cone == 0.0) {
+            factor = sqrt(lat2) * P.multiplier;
+        } else {
+            factor = sqrt(lat2 + f2 * f2) * P.multiplier;
+            const double th = fabs(M_PI / 2 - atan2(f2, sqrt(lat2)));
+            factor /= P.cone == M_PI ? 2 * M_PI : conebeam_kfactor(th, P.cone, P.soft);
+        }
+        factor *= sinc(f0) * sinc(f1) * sinc(f2);
+        if (e == 0) factor = 0.0;
+        const float2 z = P.spec[e];
+        P.spec[e] = make_float2((float)((double)z.x * factor), (float)((double)z.y * factor));
+    }
+}
+
+// out[x][y][z] += trilinear value of low at (x, y, z) / d - 1/2 + 1/(2d) per
+// axis, neighbour indices clamped to the array (scipy.ndimage.map_coordinates
+// order 1, mode "nearest", the reference's low-resolution correction,
+// filters.py:403-455). Both arrays C order (z fastest).
+__global__ void __launch_bounds__(kGThreads) k_add_upsampled(float *out, int n0, int n1, int n2, const float *low,
+                                                             int m0, int m1, int m2, int d) {
+    const int64_t n = (int64_t)n0 * n1 * n2;
+    const int64_t step = (int64_t)gridDim.x * kGThreads;
+    for (int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x; e < n; e += step) {
+        const int z = (int)(e % n2);
+        const int64_t r = e / n2;
+        const int y = (int)(r % n1), x = (int)(r / n1);
+        const int idx[3] = {x, y, z}, lim[3] = {m0, m1, m2};
+        int i0[3], i1[3];
+        double t[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double c = (double)idx[a] / d - 0.5 + 1.0 / d / 2;
+            const double f = floor(c);
+            t[a] = c - f;
+            const int fi = (int)f;
+            i0[a] = min(max(fi, 0), lim[a] - 1);
+            i1[a] = min(max(fi + 1, 0), lim[a] - 1);
+        }
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int a = c >> 2 & 1, b = c >> 1 & 1, g = c & 1;
+            const double w = (a ? t[0] : 1 - t[0]) * (b ? t[1] : 1 - t[1]) * (g ? t[2] : 1 - t[2]);
+            const int ix = a ? i1[0] : i0[0], iy = b ? i1[1] : i0[1], iz = g ? i1[2] : i0[2];
+            v += w * (double)low[((int64_t)ix * m1 + iy) * m2 + iz];
+        }
+        out[e] += (float)v;
+    }
+}
+
+unsigned grid_for(int64_t n) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+    const int64_t want = (n + kGThreads - 1) / kGThreads, cap = (int64_t)sms * 16;
+    return (unsigned)(want < cap ? want : cap);
+}
+
+bool finite_soft(const aprict_backproject_config *c) {
+    return std::isfinite(c->soft_vartheta_v) && std::isfinite(c->soft_vartheta_v_softspan) &&
+           std::isfinite(c->soft_vartheta_h) && std::isfinite(c->soft_vartheta_h_softspan);
+}
+
+}  // namespace
+
+extern "C" int aprict_b200_backproject_gbc(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                           const float *projs_dev, const aprict_vol_desc *vd, float *vol_dev,
+                                           float *weightsum_dev, const float *multiplier_dev,
+                                           const aprict_backproject_config *cfg, uint32_t *status_dev,
+                                           aprict_stream_t stream) {
+    if (cfg == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null backproject config");
+    if (cfg->weighting_preset != 7)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "the GBC backprojection takes weighting preset 7");
+    if (cfg->exact) return ab_fail(APRICT_ERR_UNSUPPORTED, "the GBC backprojection is a fast (approximate) mode");
+    if (!(cfg->Z_on_val_factor_val > 0.f) || !finite_soft(cfg))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "GBC needs R > 0 in Z_on_val_factor_val and finite soft windows");
+    if (weightsum_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "GBC needs a weight-sum volume");
+    if ((reinterpret_cast<uintptr_t>(weightsum_dev) & 3u) != 0)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "weight-sum volume pointer not 4-byte aligned");
+    if (weightsum_dev == vol_dev) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "the weight sums need their own volume");
+    aprict_backproject_config c = *cfg;
+    c.weighting_preset = 0;  // validated here; the shared checks below know presets 0-6
+    ab_bp::BPParams P;
+    uint64_t units = 0;
+    int xb = 2;
+    int rc = ab_bp::make_bp_params(specs_dev, pd, projs_dev, vd, vol_dev, multiplier_dev, &c, status_dev, P, units,
+                                   xb, 2);
+    if (rc != APRICT_OK || units == 0) return rc;
+    GbcParams G;
+    G.vol2 = weightsum_dev;
+    G.R = cfg->Z_on_val_factor_val;
+    G.soft = GbcSoft{cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan, cfg->soft_vartheta_h,
+                     cfg->soft_vartheta_h_softspan};
+    G.pos000[0] = vd->corner.x + 0.5f * vd->voxwid;
+    G.pos000[1] = vd->corner.y + 0.5f * vd->voxwid;
+    G.pos000[2] = vd->corner.z + 0.5f * vd->voxwid;
+    const int64_t nvox = (int64_t)vd->nx * vd->ny * vd->nz;
+    const int64_t blocks = (nvox + kGThreads - 1) / kGThreads;
+    if (blocks > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int order_f = vd->order != 0;
+    if (cfg->approx_mode_linear_interpolate)
+        k_backproject_gbc<true><<<(unsigned)blocks, kGThreads, 0, st>>>(P, G, order_f);
+    else
+        k_backproject_gbc<false><<<(unsigned)blocks, kGThreads, 0, st>>>(P, G, order_f);
+    return ab_cuda_check(cudaGetLastError(), "backproject_gbc launch");
+}
+
+extern "C" int aprict_b200_gbc_weight_integral(const float *r_on_R_dev, int32_t n_r, double *out_dev, int32_t num_z,
+                                               int32_t num_ang, const aprict_backproject_config *cfg,
+                                               aprict_stream_t stream) {
+    if (cfg == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null backproject config");
+    if (n_r <= 0) return APRICT_OK;
+    if (r_on_R_dev == nullptr || out_dev == nullptr)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null radius or output array");
+    if (num_z < 2 || num_ang < 1 || (int64_t)num_z * num_ang > (int64_t)1 << 31)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "num_z must be >= 2, num_ang >= 1, num_z * num_ang <= 2^31");
+    if (!finite_soft(cfg)) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "non-finite soft windows");
+    const GbcSoft S{cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan, cfg->soft_vartheta_h,
+                    cfg->soft_vartheta_h_softspan};
+    const int64_t n = (int64_t)num_z * num_ang;
+    k_gbc_weight_integ<<<(unsigned)((n + kGThreads - 1) / kGThreads), kGThreads, 0,
+                         reinterpret_cast<cudaStream_t>(stream)>>>(r_on_R_dev, n_r, out_dev, num_z, num_ang, S);
+    return ab_cuda_check(cudaGetLastError(), "gbc_weight_integral launch");
+}
+
+extern "C" int aprict_b200_conebeam_spectral(void *spec_dev, int32_t n0, int32_t n1, int32_t n2, double multiplier,
+                                             double cone_angle, double theta_soft, aprict_stream_t stream) {
+    if (n0 <= 0 || n1 <= 0 || n2 <= 0) return APRICT_OK;
+    if (spec_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null spectrum");
+    if ((reinterpret_cast<uintptr_t>(spec_dev) & 7u) != 0)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "spectrum pointer not 8-byte aligned");
+    if (!(cone_angle >= 0.0 && cone_angle <= M_PI))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "cone angle must lie in [0, pi]");
+    if (!std::isfinite(multiplier) || !std::isfinite(theta_soft))
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "non-finite multiplier or softening");
+    SpecParams P{static_cast<float2 *>(spec_dev), n0, n1, n2, multiplier, cone_angle, theta_soft};
+    const int64_t n = (int64_t)n0 * n1 * (n2 / 2 + 1);
+    k_conebeam_spectral<<<grid_for(n), kGThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(P);
+    return ab_cuda_check(cudaGetLastError(), "conebeam_spectral launch");
+}
+
+extern "C" int aprict_b200_add_upsampled(float *out_dev, int32_t n0, int32_t n1, int32_t n2, const float *low_dev,
+                                         int32_t m0, int32_t m1, int32_t m2, int32_t factor, aprict_stream_t stream) {
+    if (n0 <= 0 || n1 <= 0 || n2 <= 0) return APRICT_OK;
+    if (out_dev == nullptr || low_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "null array");
+    if (m0 <= 0 || m1 <= 0 || m2 <= 0 || factor <= 0)
+        return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "empty low-resolution array or non-positive factor");
+    const int64_t n = (int64_t)n0 * n1 * n2;
+    k_add_upsampled<<<grid_for(n), kGThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(out_dev, n0, n1, n2,
+                                                                                          low_dev, m0, m1, m2, factor);
+    return ab_cuda_check(cudaGetLastError(), "add_upsampled launch");
+}

@@ -147,7 +147,73 @@ __global__ void k_axpy(float *__restrict__ out, const float *a, float alpha, con
         out[i] = fmaf(alpha, b[i], a[i]);
 }
 
+// out = a / (w + eps exp(-w / eps)) (divide_surfaces_softzero,
+// texture_operations.cu:333-351): the reciprocal of the softened divisor,
+// then the product, in the reference's order; eps <= 0 divides plainly.
+__global__ void k_div_softzero(float *out, const float *a, const float *__restrict__ w, int64_t n, float eps) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float d = w[i];
+        if (eps > 0.f) d = d + eps * expf(-d / eps);
+        out[i] = a[i] * (1.f / d);
+    }
+}
+
+// v[x][y][z] *= g[x * ny + y] for every z (multiply_surfaces with the second
+// surface broadcast over z, texture_operations.cu:309-331).
+__global__ void k_mul_xygrid(float *v, int nx, int ny, int nz, int64_t sx, int64_t sy, int64_t sz, int order_f,
+                             const float *__restrict__ g) {
+    const int64_t n = (int64_t)nx * ny * nz;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        int x, y, z;
+        if (order_f) {  // x fastest
+            x = (int)(e % nx);
+            y = (int)((e / nx) % ny);
+            z = (int)(e / ((int64_t)nx * ny));
+        } else {  // z fastest
+            z = (int)(e % nz);
+            y = (int)((e / nz) % ny);
+            x = (int)(e / ((int64_t)ny * nz));
+        }
+        v[(int64_t)x * sx + (int64_t)y * sy + (int64_t)z * sz] *= g[(int64_t)x * ny + y];
+    }
+}
+
 }  // namespace
+
+extern "C" int aprict_b200_vol_div_softzero(float *out_dev, const float *a_dev, const float *w_dev, int64_t n,
+                                            float eps, aprict_stream_t stream) {
+    if (n < 0) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "vol_div_softzero: negative length");
+    if (n == 0) return APRICT_OK;
+    if (!a_dev || !w_dev || !out_dev) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "vol_div_softzero: null pointer");
+    if (!(eps == eps)) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "vol_div_softzero: eps is NaN");
+    k_div_softzero<<<grid_for(n), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(out_dev, a_dev, w_dev, n,
+                                                                                         eps);
+    return ab_cuda_check(cudaGetLastError(), "vol_div_softzero");
+}
+
+extern "C" int aprict_b200_vol_mul_xygrid(float *v_dev, const aprict_vol_desc *vd, const float *grid_dev,
+                                          aprict_stream_t stream) {
+    int rc = ab_check_vol(vd, v_dev, "vol_mul_xygrid");
+    if (rc != APRICT_OK) return rc;
+    const int64_t n = (int64_t)vd->nx * vd->ny * vd->nz;
+    if (n == 0) return APRICT_OK;
+    if (grid_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "vol_mul_xygrid: null grid");
+    int64_t sx, sy, sz;
+    if (vd->order == 0) {
+        sx = (int64_t)vd->ny * vd->nz;
+        sy = vd->nz;
+        sz = 1;
+    } else {
+        sx = 1;
+        sy = vd->nx;
+        sz = (int64_t)vd->nx * vd->ny;
+    }
+    k_mul_xygrid<<<grid_for(n), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        v_dev, (int)vd->nx, (int)vd->ny, (int)vd->nz, sx, sy, sz, vd->order != 0, grid_dev);
+    return ab_cuda_check(cudaGetLastError(), "vol_mul_xygrid");
+}
 
 extern "C" int aprict_b200_vol_fill(float *v_dev, int64_t n, float value, aprict_stream_t stream) {
     return launch_map(v_dev, n, FillOp{value}, stream, "vol_fill");

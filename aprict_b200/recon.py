@@ -20,12 +20,24 @@ sin^2(zeta/2) normalisation, direct-raycast backprojection with weighting
 preset 0 and (Z/R)^-3 (one-sided) or presets 1 and 6 with (Z/R)^-1 on the
 ramp- and Hilbert-filtered data (two-sided), and the scale
 (zs_max - zs_min) / (16 pi^2 R^2 M).
+
+``gbc_cone_cyl`` is the GBC reconstruction of ``aprict recon gbc``
+(src/aprict/scripts/recon_cbfp_cyl_gbc.py:371-1380): a padded volume and a
+coarse (factor n) padded volume are backprojected with the GBC weights
+(weighting preset 7) into the volume and its weight sums, scaled by
+1/(mu R^2), the weight sums normalised by their expected value over a perfect
+cylindrical locus, the volumes divided by the soft-zeroed weight sums, the
+coarse volume filtered padded and unpadded to form a low-frequency
+correction, the volume filtered with that correction added, its DC level
+estimated on the boundary and subtracted, and the padding cropped.
 """
 
 from __future__ import annotations
 
 import numpy as np
 import torch
+
+import math
 
 from .cb import flatpanel as fp
 from .cb.ramp_filter import FBPFilterer
@@ -213,3 +225,128 @@ def fbp_cone_cyl(
             o.mul_(scale)
             fp.backproject(cfg, volume, fp.ProjectionSet(pg.sliced(sl), data=o))
     return volume
+
+
+def gbc_cone_cyl(
+    projs: fp.ProjectionSet,
+    volshape: tuple[int, int, int],
+    voxwid: float,
+    volpos: tuple[float, float, float] = (0.0, 0.0, 0.0),
+    *,
+    n: int = 9,
+    f1: float = 1.2,
+    f2: float = 6.0,
+    eps: float = 1e-6,
+    softspan_v: float = 0.05,
+    softspan_h: float = 0.05,
+    interpolate_measurements: bool = True,
+    ssx: int = 1,
+    ssy: int = 1,
+    ssz: int = 1,
+    num_projs_per_chunk: int = 64,
+    num_z_samps: int = 6000,
+    num_ang_samps: int = 6000,
+) -> Volume:
+    """GBC reconstruction of ``projs`` (M, nu, nv) from a cylindrical source
+    locus into a new (``volshape``, ``voxwid``, ``volpos``) volume.
+
+    Options follow the reference's CLI (recon_cbfp_cyl_gbc.py:166-240): ``n``
+    (odd) the coarse volume's downscale factor, ``f1`` / ``f2`` the padding
+    factors of the full and coarse volumes, ``eps`` the soft-zero of the
+    weight division, ``softspan_v`` / ``softspan_h`` the soft window spans.
+    The reference processes the volumes in z slabs to fit device memory;
+    here each volume is one array (the result is the same: every step is
+    per voxel, and the filters act on the whole arrays in both).
+    """
+    from .gbc import filters, weightinteg  # noqa: PLC0415
+
+    if projs.data is None:
+        msg = "You must provide projection data."
+        raise ValueError(msg)
+    if n < 1 or n % 2 == 0:
+        msg = "n must be a positive odd integer."
+        raise ValueError(msg)
+    if min(ssx, ssy, ssz) <= 0:
+        msg = "ssx, ssy, ssz must all be positive integers."
+        raise ValueError(msg)
+    volshape = tuple(int(s) for s in volshape)
+    # padded shapes (recon_cbfp_cyl_gbc.py:649-684)
+    padded = tuple(n * (4 + math.ceil(s * f1 / n)) for s in volshape)
+    padded = tuple(p if (p - s) % 2 == 0 else p + n for s, p in zip(volshape, padded))
+    pads = tuple((p - s) // 2 for s, p in zip(volshape, padded))
+    mini = tuple(math.ceil(s * f2 / n) for s in volshape)
+    mini = tuple(max(m, p // n) for p, m in zip(padded, mini))
+    mini = tuple(m if (m - p // n) % 2 == 0 else m + 1 for p, m in zip(padded, mini))
+    mpads = tuple((m - p // n) // 2 for p, m in zip(padded, mini))
+
+    vol = Volume.zeros(padded, voxwid=voxwid, pos_c=volpos)
+    vol_ws = Volume.zeros(padded, voxwid=voxwid, pos_c=volpos)
+    minivol = Volume.zeros(mini, voxwid=voxwid * n, pos_c=volpos)
+    minivol_ws = Volume.zeros(mini, voxwid=voxwid * n, pos_c=volpos)
+
+    # geometry (recon_cbfp_cyl_gbc.py:371-534)
+    pg = projs.proj_geom
+    R, L, pixwid, nu, nv = fan_geometry(pg)  # noqa: N806
+    m = pg.num_projs
+    vartheta_v = float(np.arctan2(nv * pixwid / 2 - pixwid / 2, np.sqrt(L**2 + (nu * pixwid / 2 - pixwid / 2) ** 2)))
+    vartheta_h = float(np.arctan2(nu * pixwid / 2 - pixwid / 2, L))
+    src_z = np.broadcast_to(pg.source_pos, pg.projs_list_shape + (3,))[:, 2].astype(np.float64)
+    zs_max, zs_min = float(src_z.max()), float(src_z.min())
+    (x0, y0, z0), (x1, y1, z1) = minivol.minxyz_maxxyz
+    max_r = float(np.sqrt(max(abs(x0), abs(x1)) ** 2 + max(abs(y0), abs(y1)) ** 2))
+    hdiff = np.tan(vartheta_v) * (R + max_r)
+    mu = m / (2 * np.pi * R * (zs_max - zs_min))
+    cfg = fp.ConfigBackproject(
+        fast_approx=True, Z_on_val_factor_val=R, backproj_weighting_preset=7, approx_mode_direct_raycast=True,
+        approx_mode_bilinear_interpolate=interpolate_measurements, ssx=ssx, ssy=ssy, ssz=ssz,
+        soft_vartheta_v=vartheta_v, soft_vartheta_v_softspan=softspan_v, soft_vartheta_h=vartheta_h,
+        soft_vartheta_h_softspan=softspan_h,
+    )
+
+    def divisor(v: Volume) -> np.ndarray:
+        xs, ys, _ = v.xs_ys_zs
+        integ = weightinteg.backproj_gbc_weight_integ_xygrid_GPU(xs, ys, R, cfg, num_z_samps, num_ang_samps)
+        return np.power(integ, -1).astype(np.float32)
+
+    div_full, div_mini = divisor(vol), divisor(minivol)
+
+    # backprojection of every chunk of views within reach of the volumes (:1104-1190)
+    done = 0
+    for a in range(0, m, num_projs_per_chunk):
+        sl = slice(a, min(m, a + num_projs_per_chunk))
+        if z1 < src_z[sl].min() - hdiff or z0 > src_z[sl].max() + hdiff:
+            continue
+        ps = fp.ProjectionSet(pg.sliced(sl), data=projs.data[sl])
+        fp.backproject(cfg, vol, ps, secondary_volume=vol_ws)
+        fp.backproject(cfg, minivol, ps, secondary_volume=minivol_ws)
+        done += sl.stop - sl.start
+    if done > 0:  # (:1191-1222)
+        factor = 1 / (mu * R**2)
+        for v in (vol, vol_ws, minivol, minivol_ws):
+            v.multiply(factor)
+        vol_ws.multiply_by_xygrid(div_full)
+        minivol_ws.multiply_by_xygrid(div_mini)
+        vol.divide_softzero(vol_ws, eps=eps)
+        minivol.divide_softzero(minivol_ws, eps=eps)
+    del vol_ws, minivol_ws
+
+    # filtering with the low-frequency correction (:1245-1324)
+    cone = 2 * vartheta_v
+    crop_m = tuple(slice(p, (-p) or None) for p in mpads)
+    mini_pad_f = filters.ramp_filter_conebeam(minivol.data, voxwid * n, cone, theta_soft=softspan_v)
+    mini_unpad_f = filters.ramp_filter_conebeam(minivol.data[crop_m].contiguous(), voxwid * n, cone,
+                                                theta_soft=softspan_v)
+    correction = mini_pad_f[crop_m] - mini_unpad_f
+    del mini_pad_f, mini_unpad_f, minivol
+    out = filters.ramp_filter_conebeam(vol.data, voxwid, cone, theta_soft=softspan_v,
+                                       lowres_correction_array=correction.contiguous())
+    del vol, correction
+    # DC level from the boundary of the central region (:1326-1352)
+    c = out[2 * n : -2 * n, 2 * n : -2 * n, 2 * n : -2 * n]
+    dc = 0.25 * (c[:, 0, :].double().mean() + c[:, -1, :].double().mean() + c[0, :, :].double().mean()
+                 + c[-1, :, :].double().mean())
+    out -= dc.float()
+    crop = tuple(slice(p, (-p) or None) for p in pads)
+    res = Volume.zeros(volshape, voxwid=voxwid, pos_c=volpos)
+    res.data.copy_(out[crop])
+    return res

@@ -180,6 +180,33 @@ class Volume:
             "Volume.multiply_volume",
         )
 
+    def divide(self, other: Volume) -> None:
+        """Element-wise division by another volume (divide_textures)."""
+        self.divide_softzero(other, eps=0.0)
+
+    def divide_softzero(self, other: Volume, eps: float) -> None:
+        """self <- self / (other + eps exp(-other / eps)) (volume.py:196-200,
+        divide_surfaces_softzero); eps <= 0 divides plainly."""
+        self._check_same(other)
+        _lib.check(
+            _lib.lib().aprict_b200_vol_div_softzero(
+                self._data.data_ptr(), self._data.data_ptr(), other._data.data_ptr(), self._numel, float(eps), _stream()
+            ),
+            "Volume.divide_softzero",
+        )
+
+    def multiply_by_xygrid(self, xygrid: np.ndarray | torch.Tensor) -> None:
+        """Multiply in place by an (nx, ny) grid broadcast over z (volume.py:170-190)."""
+        g = torch.as_tensor(xygrid, dtype=torch.float32).to(self._data.device).contiguous()
+        if tuple(g.shape) != tuple(self._shape[:2]):
+            msg = "Input array should be 2-dimensional and match the shape[:2] of this volume."
+            raise ValueError(msg)
+        vd = self._desc()
+        _lib.check(
+            _lib.lib().aprict_b200_vol_mul_xygrid(self._data.data_ptr(), _lib.ptr(vd), g.data_ptr(), _stream()),
+            "Volume.multiply_by_xygrid",
+        )
+
     def add_scaled(self, other: Volume, alpha: float) -> None:
         """self += alpha * other."""
         self._check_same(other)

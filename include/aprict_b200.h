@@ -217,6 +217,17 @@ APRICT_API int aprict_b200_vol_mul(float *out_dev, const float *a_dev, const flo
 APRICT_API int aprict_b200_vol_axpy(float *out_dev, const float *a_dev, float alpha, const float *b_dev,
                                     int64_t n, aprict_stream_t stream);
 
+/* out = a / (w + eps exp(-w / eps)), the reciprocal taken first
+ * (divide_surfaces_softzero, texture_operations.cu:333-351); eps <= 0 divides
+ * plainly. out may alias a. */
+APRICT_API int aprict_b200_vol_div_softzero(float *out_dev, const float *a_dev, const float *w_dev, int64_t n,
+                                            float eps, aprict_stream_t stream);
+
+/* v[x][y][z] *= grid[x * ny + y] for every z (Volume.multiply_by_xygrid,
+ * volume.py:170-190). */
+APRICT_API int aprict_b200_vol_mul_xygrid(float *v_dev, const aprict_vol_desc *vd, const float *grid_dev,
+                                          aprict_stream_t stream);
+
 /* ---- Ramp filtering ----
  * out[view][m][v] = scale * sum_j taps[m - j + nu - 1] * w[j][v] * in[view][j][v]
  * for m, j in [0, nu): the linear convolution the reference evaluates by
@@ -253,6 +264,48 @@ APRICT_API int aprict_b200_rotate_projections(const aprict_proj_desc *in, const 
                                               double centre_u, double centre_v, int32_t in_off_u, int32_t in_off_v,
                                               int32_t out_off_u, int32_t out_off_v, const double *mask_dev,
                                               const double *colw_dev, aprict_stream_t stream);
+
+/* ---- GBC reconstruction ---- */
+
+/* GBC backprojection with a cylindrical source locus
+ * (backproject_CB_voltex_GBC_cyl, CB_backproject.cu:736-905, 1030-1105; chosen
+ * by flatpanel.backproject for weighting preset 7, flatpanel.py:216-232).
+ * For every voxel and view: the weight w of _GBC_weightfun (R =
+ * cfg->Z_on_val_factor_val, about the world z axis; soft windows from the
+ * soft_vartheta_* fields), weightsum += w and, where w != 0, vol += w times
+ * the nearest or bilinear detector value; both sums averaged over the
+ * ssx*ssy*ssz sub-samples and multiplied by the summand multiplier. No
+ * cylinder mask, taper or Z factors. cfg->weighting_preset must be 7;
+ * weightsum_dev has the volume's layout and must not alias it. */
+APRICT_API int aprict_b200_backproject_gbc(const aprict_proj_spec *specs_dev, const aprict_proj_desc *pd,
+                                           const float *projs_dev, const aprict_vol_desc *vd, float *vol_dev,
+                                           float *weightsum_dev, const float *multiplier_dev,
+                                           const aprict_backproject_config *cfg, uint32_t *status_dev,
+                                           aprict_stream_t stream);
+
+/* out_dev[r] += the expected GBC weight sum at radius r_on_R_dev[r] (units of
+ * R, increasing) over a perfect cylindrical locus sampled by num_z heights and
+ * num_ang angles (get_GBC_weight_integ, CB_backproject.cu:1108-1168;
+ * gbc/weightinteg.py:22-57). The caller zeroes out_dev (FP64). */
+APRICT_API int aprict_b200_gbc_weight_integral(const float *r_on_R_dev, int32_t n_r, double *out_dev, int32_t num_z,
+                                               int32_t num_ang, const aprict_backproject_config *cfg,
+                                               aprict_stream_t stream);
+
+/* In place on the (n0, n1, n2/2+1) complex64 rfftn spectrum of an (n0, n1,
+ * n2) volume (axis 2 the cylinder axis): times multiplier * |k|, divided by
+ * the softened Colsher k-factor of the polar angle (cone_angle in (0, pi);
+ * 2 pi at cone_angle = pi; lateral |k| and no k-factor at cone_angle = 0),
+ * times sinc(f0) sinc(f1) sinc(f2), DC set to 0 (ramp_filter_conebeam,
+ * gbc/filters.py:59-147, 340-398). */
+APRICT_API int aprict_b200_conebeam_spectral(void *spec_dev, int32_t n0, int32_t n1, int32_t n2, double multiplier,
+                                             double cone_angle, double theta_soft, aprict_stream_t stream);
+
+/* out[x][y][z] += order-1 interpolation of low (m0, m1, m2) at
+ * (x, y, z) / factor - 1/2 + 1/(2 factor), neighbour indices clamped
+ * (map_coordinates mode "nearest"; the low-resolution correction of
+ * ramp_filter_conebeam, gbc/filters.py:403-455). Both C order. */
+APRICT_API int aprict_b200_add_upsampled(float *out_dev, int32_t n0, int32_t n1, int32_t n2, const float *low_dev,
+                                         int32_t m0, int32_t m1, int32_t m2, int32_t factor, aprict_stream_t stream);
 
 /* ---- Analytic (FORBILD) phantoms ---- */
 

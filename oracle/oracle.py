@@ -307,6 +307,58 @@ def ref_backproject(
     return vol
 
 
+def ref_backproject_gbc(
+    specs: np.ndarray,
+    projs: np.ndarray,
+    vol: np.ndarray,
+    vol2: np.ndarray,
+    cfg_contents: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    mult: np.ndarray | None = None,
+    nthreads: int | None = None,
+) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's backproject_CB_voltex_GBC_cyl<float,float> on the CPU; accumulates into
+    ``vol`` and the weight sums into ``vol2`` (both C order float32)."""
+    lib = _load(REF_SO)
+    lib.ref_backproject_gbc.restype = ctypes.c_longlong
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    p = np.ascontiguousarray(projs, dtype=np.float32)
+    for v in (vol, vol2):
+        if not (v.flags["C_CONTIGUOUS"] and v.dtype == np.float32):
+            msg = "volumes must be C-contiguous float32 arrays"
+            raise ValueError(msg)
+    mm = None if mult is None else np.ascontiguousarray(mult, dtype=np.float32)
+    c = cfg_contents
+    soft = np.array([c["soft_vartheta_v"], c["soft_vartheta_v_softspan"], c["soft_vartheta_h"],
+                     c["soft_vartheta_h_softspan"]], dtype=np.float32)
+    tp = np.asarray(corner, dtype=np.float32)
+    f = ctypes.c_float
+    oob = lib.ref_backproject_gbc(
+        _p(s), m, nu, nv, _p(p), _p(vol), _p(vol2), vol.shape[0], vol.shape[1], vol.shape[2], f(voxwid), _p(tp),
+        None if mm is None else _p(mm), f(float(c["Z_on_val_factor_val"])), int(c["approx_mode_linear_interpolate"]),
+        int(c["ssx"]), int(c["ssy"]), int(c["ssz"]), _p(soft), nthreads or nthreads_default(),
+    )
+    if oob:
+        msg = f"reference GBC backprojector accessed outside the volume {oob} times"
+        raise RuntimeError(msg)
+    return vol, vol2
+
+
+def ref_gbc_weight(R: float, vox: np.ndarray, src: np.ndarray, soft: np.ndarray) -> np.ndarray:  # noqa: N803
+    """The reference's _GBC_weightfun<float> at points vox (n, 3) for sources src (n, 3);
+    soft = (vartheta_v, span_v, vartheta_h, span_h)."""
+    lib = _load(REF_SO)
+    v = np.ascontiguousarray(vox, dtype=np.float32)
+    s = np.ascontiguousarray(src, dtype=np.float32)
+    so = np.ascontiguousarray(soft, dtype=np.float32)
+    out = np.empty(len(v), np.float32)
+    lib.ref_gbc_weight(ctypes.c_float(R), _p(v), _p(s), _p(so), ctypes.c_longlong(len(v)), _p(out))
+    return out
+
+
 # --------------------------------------------------------------------- FORBILD shapes
 def project_forbild(
     specs: np.ndarray,

@@ -112,12 +112,30 @@ def test_backproject_validation() -> None:
     cfg = fp.ConfigBackproject(apply_summand_multiplier=True).contents
     rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
     assert rc == 1
-    # weighting preset 7 (the GBC formula) is not implemented
+    # weighting preset 7 (GBC) has its own entry point
     cfg = fp.ConfigBackproject(backproj_weighting_preset=7).contents
     rc = lib.aprict_b200_backproject(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), None, _lib.ptr(cfg), None, None)
     assert rc == 2
     with pytest.raises(NotImplementedError):
         _lib.check(rc, "backproject")
+    gbc = fp.ConfigBackproject(fast_approx=True, backproj_weighting_preset=7, Z_on_val_factor_val=100.0,
+                               soft_vartheta_v=0.2, soft_vartheta_v_softspan=0.05, soft_vartheta_h=0.4,
+                               soft_vartheta_h_softspan=0.05).contents
+    bad = [
+        (fp.ConfigBackproject(fast_approx=True).contents, _fake() + 4096),       # preset 0
+        (fp.ConfigBackproject(backproj_weighting_preset=7, Z_on_val_factor_val=100.0).contents, _fake() + 4096),  # exact
+        (gbc, None),                                                             # no weight-sum volume
+        (gbc, _fake()),                                                          # aliases the volume
+        (gbc, _fake() + 2),                                                      # unaligned
+    ]
+    for c, ws in bad:
+        rc = lib.aprict_b200_backproject_gbc(_fake(), _lib.ptr(pd), _fake(), _lib.ptr(vd), _fake(), ws, None,
+                                             _lib.ptr(c), None, None)
+        assert rc in (1, 2)
+    assert lib.aprict_b200_conebeam_spectral(_fake(), 4, 4, 4, ctypes.c_double(1.0), ctypes.c_double(4.0),
+                                             ctypes.c_double(0.1), None) == 1  # cone angle > pi
+    assert lib.aprict_b200_gbc_weight_integral(_fake(), 3, _fake(), 1, 10, _lib.ptr(gbc), None) == 1  # num_z < 2
+    assert lib.aprict_b200_vol_div_softzero(None, _fake(), _fake(), 10, ctypes.c_float(1e-6), None) == 1
 
 
 def test_volops_validation() -> None:
