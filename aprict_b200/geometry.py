@@ -42,6 +42,33 @@ def helical_scan(
     return fp.ProjGeom(source_pos=src, det_pos=det, det_uvec=u, det_vvec=v, nu=nu, nv=nv)
 
 
+def cylinder_scan(
+    *,
+    n_views: int,
+    R: float,  # noqa: N803
+    L_minus_R: float,  # noqa: N803
+    pix_at_iso: float,
+    nu: int,
+    nv: int,
+    height: float,
+    theta_start: float = 0.0,
+    clockwise: bool = False,
+) -> fp.ProjGeom:
+    """Source points on a cylinder of radius R: heights evenly spaced over
+    (-height/2, height/2) (ends excluded), angles stepping by the golden angle
+    (sqrt(5) - 1) pi -- the GOLDEN_THETA trajectory of the reference's
+    cone-cylinder geometry maker (scripts/make_geometry_cone_cyl.py:233-289)."""
+    mag = (R + L_minus_R) / R
+    pix = pix_at_iso * mag
+    zs = np.linspace(-height / 2, height / 2, num=n_views + 2, endpoint=True)[1:-1]
+    ts = theta_start + (-1 if clockwise else 1) * np.arange(n_views, dtype=np.float64) * (np.sqrt(5) - 1) * np.pi
+    src = np.stack([R * np.cos(ts), R * np.sin(ts), zs], axis=1)
+    det = np.stack([-L_minus_R * np.cos(ts), -L_minus_R * np.sin(ts), zs], axis=1)
+    u = pix * np.stack([-np.sin(ts), np.cos(ts), 0 * ts], axis=1)
+    v = np.broadcast_to(pix * np.array([0.0, 0.0, -1.0]), (n_views, 3)).copy()
+    return fp.ProjGeom(source_pos=src, det_pos=det, det_uvec=u, det_vvec=v, nu=nu, nv=nv)
+
+
 def jitter_views(rng: np.random.Generator, pg: fp.ProjGeom, mm: float = 2.0, deg: float = 0.5) -> fp.ProjGeom:
     """Per view: source and detector moved by up to +-mm along each axis, and
     the detector's u and v turned together (staying orthogonal) by up to +-deg

@@ -54,6 +54,14 @@ WORKLOADS = {
     #   720 views on 1024^2 x 0.3 mm, SOD 700, SDD 1200, additive densities.
     "fpbp128": dict(n=128, voxwid=1.0, n_ellipsoids=10, views=180, det=256, pix_at_iso=0.5, R=500.0, LmR=500.0, seed=3),
     "fbp64": dict(slices=64, n=512, voxwid=0.5, n_ellipses=20, views=720, det=1024, pix=0.4, R=600.0, LmR=500.0, seed=7),
+    # fbpcyl -- cone-cylinder FBP: 256^3 x 0.5 mm, 720 golden-angle views on a 500 mm cylinder
+    #   (80 mm high) x 384^2 x 0.8 mm, tilted filtering + direct-raycast backprojection;
+    # gbc -- GBC reconstruction: 128^3 x 1 mm, 360 views on a 500 mm cylinder (128 mm high)
+    #   x 256^2 x 1.5 mm, n = 9, f1 = 1.2, f2 = 6, 6000 x 6000 weight-integral samples.
+    "fbpcyl": dict(n=256, voxwid=0.5, n_ellipsoids=30, views=720, det=384, pix_at_iso=0.4, R=500.0, LmR=500.0,
+                   height=80.0, seed=11),
+    "gbc": dict(n=128, voxwid=1.0, n_ellipsoids=20, views=360, det=256, pix_at_iso=0.75, R=500.0, LmR=500.0,
+                height=128.0, seed=12),
     "quadric": dict(n_ellipsoids=60, n_cylinders=40, radius=100.0, views=720, det=1024, pix=0.3, R=700.0, LmR=500.0,
                     seed=11),
     "batch48": dict(n_scans=48, edge=(64, 320), views=(90, 720), det=(128, 768), voxwid=0.5, n_ellipsoids=10,
@@ -721,6 +729,8 @@ def run_component(args) -> dict:
                                 "filtered_samples_per_s": round(S * m * nu / (t_b * 1e-3), 1)}}
         return _line(args, "fan FBP slices/s", round(S / (t_b * 1e-3), 2), "slices/s", t_b,
                      f"fbp64: {S} slices {n}^2 x {w['voxwid']} mm, {m} views x {nu} x {w['pix']} mm, Ram-Lak + Hann", extra)
+    if args.workload in ("fbpcyl", "gbc"):
+        return _run_cylinder_recon(args, w)
     # quadric
     shapes = phantoms.random_quadric_phantom(w["seed"], n_ellipsoids=w["n_ellipsoids"], n_cylinders=w["n_cylinders"],
                                              radius=w["radius"])
@@ -739,6 +749,95 @@ def run_component(args) -> dict:
                             "output_write_GBps": round(4 * rays / (t_q * 1e-3) / 1e9, 1)}}
     return _line(args, "quadric projection rays/s", round(rays / (t_q * 1e-3), 1), "rays/s", t_q,
                  f"quadric: {len(shapes)} clipped quadrics in {2 * w['radius']:.0f} mm, {w['views']} views x {w['det']}^2 x {w['pix']} mm, additive", extra)
+
+
+def _run_cylinder_recon(args, w: dict) -> dict:
+    """The fbpcyl and gbc workloads: one full reconstruction per step, with its parts timed apart."""
+    import torch  # noqa: F401
+
+    from aprict_b200 import Volume, geometry, phantoms
+    from aprict_b200.cb import flatpanel as fp
+    from aprict_b200.cb.ramp_filter import FBPFilterer
+    from aprict_b200.gbc import weightinteg
+    from aprict_b200.recon import fan_geometry, fbp_cone_cyl, gbc_cone_cyl
+
+    n, vw, m = w["n"], w["voxwid"], w["views"]
+    pg = geometry.cylinder_scan(n_views=m, R=w["R"], L_minus_R=w["LmR"], pix_at_iso=w["pix_at_iso"], nu=w["det"],
+                                nv=w["det"], height=w["height"])
+    x = Volume(phantoms.ellipsoid_volume(w["seed"], w["n_ellipsoids"], (n, n, n), vw, semi_axes_vox=(3, n / 5)),
+               voxwid=vw)
+    ps = fp.ProjectionSet(pg, data=None)
+    fp.project(fp.ConfigProject(), x, ps, block=True)
+    R, L, pixwid, nu, nv = fan_geometry(pg)  # noqa: N806
+    steps = max(1, args.steps)
+
+    if args.workload == "fbpcyl":
+        out = Volume.zeros((n, n, n), voxwid=vw)
+        t_all = _timed(lambda: fbp_cone_cyl(ps, out, seed_proj_rots=1, num_projs_per_chunk=m), steps)
+        filt = FBPFilterer(L=L, physpixwid=pixwid, proj_2d_shape=(nu, nv), projs_per_batch=m,
+                           rng=np.random.default_rng(1))
+        t_f = _timed(lambda: filt.filter_bulk_axis1_concat(ps.data, block=False), steps)
+        (filtered,), _ = filt.filter_bulk_axis1_concat(ps.data)
+        support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
+        cfg = fp.ConfigBackproject(fast_approx=True, cyl_mask_rad=support, Z_on_val_factor_power=-3,
+                                   Z_on_val_factor_val=R, approx_mode_direct_raycast=True)
+        fps = fp.ProjectionSet(pg, data=filtered)
+        t_bp = _timed(lambda: fp.backproject(cfg, out, fps), steps)
+        vv = n**3 * m
+        extra = {"components": {"recon_ms": round(t_all, 3), "tilted_filter_ms": round(t_f, 3),
+                                "backproject_ms": round(t_bp, 3),
+                                "back_voxel_updates_per_s": round(vv / (t_bp * 1e-3), 1),
+                                "filtered_views_per_s": round(m / (t_f * 1e-3), 1)}}
+        from oracle import oracle  # the CPU baseline leg
+
+        if not args.no_cpu_baseline and oracle.have_ref():
+            sel = np.linspace(0, m, 4, endpoint=False).astype(int)
+            corner = -np.float32(vw) * np.array((n, n, n), np.float32) / 2
+            v = np.zeros((n, n, n), np.float32)
+            f_host = filtered.cpu().numpy()[sel]
+            t0 = time.perf_counter()
+            oracle.ref_backproject(pg.to_proj_spec_array()[sel], f_host, v, cfg.contents, voxwid=vw, corner=corner)
+            dt = time.perf_counter() - t0
+            extra["cpu_baseline"] = {"value": round(len(sel) * n**3 / dt, 1), "unit": "voxel-updates/s",
+                                     "cores": os.cpu_count() or 1, "kind": "reference",
+                                     "sample": f"direct-raycast backprojection of {len(sel)} of {m} views "
+                                               "(the reference's filter runs on the GPU through cupyx: no CPU arm)"}
+        return _line(args, "cone-cylinder FBP reconstructions/s", round(1000.0 / t_all, 3), "recon/s", t_all,
+                     f"fbpcyl: {n}^3 x {vw} mm, {m} golden-angle views on R {w['R']} mm x {w['height']} mm, "
+                     f"{nu}^2 x {pixwid:.2f} mm, one random filter rotation per view", extra)
+    # gbc
+    t_all = _timed(lambda: gbc_cone_cyl(ps, (n, n, n), vw), steps)
+    vartheta_v = float(np.arctan2(nv * pixwid / 2 - pixwid / 2, np.sqrt(L**2 + (nu * pixwid / 2 - pixwid / 2) ** 2)))
+    vartheta_h = float(np.arctan2(nu * pixwid / 2 - pixwid / 2, L))
+    cfg = fp.ConfigBackproject(fast_approx=True, Z_on_val_factor_val=R, backproj_weighting_preset=7,
+                               approx_mode_direct_raycast=True, approx_mode_bilinear_interpolate=True,
+                               soft_vartheta_v=vartheta_v, soft_vartheta_v_softspan=0.05, soft_vartheta_h=vartheta_h,
+                               soft_vartheta_h_softspan=0.05)
+    pad = 9 * (4 + int(np.ceil(n * 1.2 / 9)))
+    pad = pad if (pad - n) % 2 == 0 else pad + 9
+    vol, ws = Volume.zeros((pad,) * 3, voxwid=vw), Volume.zeros((pad,) * 3, voxwid=vw)
+    t_bp = _timed(lambda: fp.backproject(cfg, vol, ps, secondary_volume=ws), steps)
+    xs = vol.xs_ys_zs[0]
+    t_wi = _timed(lambda: weightinteg.backproj_gbc_weight_integ_xygrid_GPU(xs, xs, R, cfg), steps)
+    vv = pad**3 * m
+    extra = {"components": {"recon_ms": round(t_all, 3), "gbc_backproject_padded_ms": round(t_bp, 3),
+                            "weight_integral_ms": round(t_wi, 3), "padded_edge": pad,
+                            "gbc_voxel_updates_per_s": round(vv / (t_bp * 1e-3), 1)}}
+    from oracle import oracle  # the CPU baseline leg
+
+    if not args.no_cpu_baseline and oracle.have_ref():
+        sel = np.array([0, m // 2])
+        v1, v2 = np.zeros((pad,) * 3, np.float32), np.zeros((pad,) * 3, np.float32)
+        t0 = time.perf_counter()
+        oracle.ref_backproject_gbc(pg.to_proj_spec_array()[sel], ps.data.cpu().numpy()[sel], v1, v2, cfg.contents,
+                                   voxwid=vw, corner=vol.corner)
+        dt = time.perf_counter() - t0
+        extra["cpu_baseline"] = {"value": round(len(sel) * pad**3 / dt, 1), "unit": "voxel-updates/s",
+                                 "cores": os.cpu_count() or 1, "kind": "reference",
+                                 "sample": f"GBC backprojection of {len(sel)} of {m} views into the {pad}^3 padded volume"}
+    return _line(args, "GBC reconstructions/s", round(1000.0 / t_all, 4), "recon/s", t_all,
+                 f"gbc: {n}^3 x {vw} mm, {m} golden-angle views on R {w['R']} mm x {w['height']} mm, "
+                 f"{nu}^2 x {pixwid:.2f} mm, n 9, f1 1.2, f2 6", extra)
 
 
 def profile_kernels(args) -> dict:
@@ -814,7 +913,7 @@ def main() -> None:
             out = run_reference(args)
         elif args.workload == "batch48":
             out = run_batch(args)
-        elif args.workload in ("fpbp128", "fbp64", "quadric"):
+        elif args.workload in ("fpbp128", "fbp64", "quadric", "fbpcyl", "gbc"):
             out = run_component(args)
         else:
             out = run_ours(args)
