@@ -13,8 +13,9 @@
 // The backprojection launches once for all views (the reference: once per 10
 // views, the volume read-modified-written each time). One thread per voxel,
 // consecutive threads on consecutive voxels in memory order, per-view
-// coefficients staged in shared memory. The weight is evaluated in FP32 with
-// the CUDA math library (atan2f, cosf, acosf, sinf), the detector coordinate
+// coefficients staged in shared memory. The weight is evaluated in FP32 from
+// reciprocal square roots and one division (the angles' sines and cosines by
+// trigonometric identities, the soft windows on squared sines), the detector coordinate
 // by the same linear forms as the other backprojection modes, and the
 // nearest-pixel choice re-decided in FP64 near ties, so the result follows
 // the FP64 restatement. The spectral filter is one pass over the cuFFT
@@ -33,41 +34,69 @@ constexpr int kGThreads = 256;
 constexpr int kGChunk = 64;  // views per shared-memory chunk
 
 // Soft window s(a, b; c) of cossq_soft (CB_backproject.cu:273-311): 0 beyond
-// |c| = a, 1 inside |c| = a - b, 3x^2 - 2x^3 between, x = gamma sin|c| - chi.
-__device__ float cossq_soft(float a, float b, float c) {
-    if (fabsf(c) > a) return 0.f;
-    if (fabsf(c) < a - b) return 1.f;
-    const float gamma = 1.f / (sinf(a - b) - sinf(a));
-    const float chi = gamma * sinf(a);
-    const float x = gamma * sinf(fabsf(c)) - chi;
+// |c| = a, 1 inside |c| = a - b, 3x^2 - 2x^3 between, x = gamma sin|c| - chi,
+// gamma = 1 / (sin(a - b) - sin a), chi = gamma sin a. Both angles the weight
+// feeds it lie in [0, pi/2], where sin is increasing, so the window is taken
+// as a function of s = sin|c| with the comparisons made on sines: no
+// transcendental per voxel-view. The constants come from the host in FP64.
+struct SoftWin {
+    float sa2, sab2, gamma, chi;  // sin^2 a (4 if a >= pi/2), sin^2(a - b) (-1 if a - b <= 0, 4 if >= pi/2), gamma, chi
+};
+
+struct GbcSoft {
+    SoftWin v, h;  // vertical (elevation) and horizontal windows
+};
+
+SoftWin soft_win(double a, double b) {
+    const double half_pi = 1.5707963267948966;
+    SoftWin w;
+    w.sa2 = a >= half_pi ? 4.f : (float)(sin(a) * sin(a));
+    w.sab2 = a - b <= 0.0 ? -1.f : (a - b >= half_pi ? 4.f : (float)(sin(a - b) * sin(a - b)));
+    const double g = 1.0 / (sin(a - b) - sin(a));
+    w.gamma = (float)g;
+    w.chi = (float)(g * sin(a));
+    return w;
+}
+
+// The window at s = sqrt(s2), s = sin|angle| in [0, 1]: compared on squares,
+// a square root only inside the soft band.
+__device__ __forceinline__ float soft_of_sin2(float s2, const SoftWin &w) {
+    if (s2 > w.sa2) return 0.f;
+    if (s2 < w.sab2) return 1.f;
+    const float x = w.gamma * sqrtf(s2) - w.chi;
     return fmaxf(0.f, fminf(1.f, 3.f * x * x - 2.f * x * x * x));
 }
 
-struct GbcSoft {
-    float v, v_span, h, h_span;  // soft_vartheta_v, its span, soft_vartheta_h, its span
-};
-
 // GBC weight (eq. 23 of the GBC method with the soft windows,
 // CB_backproject.cu:736-787) of the voxel at world position p for the source
-// at s, R the radius of the source cylinder about the world z axis.
-__device__ float gbc_weight(float R, float px, float py, float pz, float sx, float sy, float sz, const GbcSoft &S) {
-    const float lx = -sx, ly = -sy;  // L = (-s_x, -s_y, 0)
+// at s (inv_ls = 1 / |(s_x, s_y)|), on a cylinder of radius R (inv_R = 1/R)
+// about the world z axis. With r = p - s, q = r_x^2 + r_y^2:
+//   ell = sqrt(q) / R, c = clamp(|Z / R / ell|) = clamp(|r . L| / (|L| sqrt(q))),
+//   theta = atan2(r_z / R, ell): cos theta = ell / h, sin|theta| = |r_z / R| / h,
+//   h = hypot(ell, r_z / R); phi = acos(c): sin^2 phi = 1 - c^2.
+// Reciprocal square roots and one fast division, as the reference's
+// fast-math build evaluates its transcendental form; the limits at q = 0 and
+// h = 0 are the reference's (c = 1, cos theta = 1).
+__device__ float gbc_weight(float inv_R, float px, float py, float pz, float sx, float sy, float sz, float inv_ls,
+                            const GbcSoft &S) {
     const float rx = px - sx, ry = py - sy, rz = pz - sz;
-    const float Z = (rx * lx + ry * ly) / sqrtf(lx * lx + ly * ly);
-    const float ell_on_R = sqrtf(rx * rx + ry * ry) / R;
-    const float Z_on_R = Z / R;
-    const float c_on_R = fmaxf(0.f, fminf(1.f, fabsf(Z_on_R / ell_on_R)));
-    const float d_on_R = c_on_R - ell_on_R;
-    const float theta_el = atan2f(rz / R, ell_on_R);
-    const float cos_el = cosf(theta_el);
-    const float weight = cos_el * cos_el * cos_el * c_on_R / fmaxf(1e-9f, c_on_R * c_on_R + d_on_R * d_on_R);
-    const float soft = cossq_soft(S.v, S.v_span, theta_el) * cossq_soft(S.h, S.h_span, acosf(c_on_R));
-    return weight * soft;
+    const float q = rx * rx + ry * ry;
+    const float rq = rsqrtf(q);
+    const float ell = q > 0.f ? q * rq * inv_R : 0.f;
+    const float c = fmaxf(0.f, fminf(1.f, fabsf((rx * sx + ry * sy) * inv_ls * rq)));  // NaN at q = 0 -> 1
+    const float d = c - ell;
+    const float zr = rz * inv_R;
+    const float h2 = ell * ell + zr * zr;
+    const float ih = rsqrtf(h2);
+    const float cos_el = h2 > 0.f ? ell * ih : 1.f;
+    const float sin2_el = h2 > 0.f ? zr * zr * (ih * ih) : 0.f;
+    const float weight = __fdividef(cos_el * cos_el * cos_el * c, fmaxf(1e-9f, c * c + d * d));
+    return weight * soft_of_sin2(sin2_el, S.v) * soft_of_sin2(fmaxf(0.f, 1.f - c * c), S.h);
 }
 
 struct GbcParams {
     float *vol2;  // weight-sum volume (same layout as the volume)
-    float R;
+    float inv_R;  // 1 / R
     GbcSoft soft;
     float pos000[3];  // world centre of voxel (0, 0, 0): corner + voxwid / 2
 };
@@ -78,7 +107,7 @@ __global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPPa
     using namespace ab_bp;
     __shared__ ab_bpview sv[kGChunk];
     __shared__ ab_bpview_d svd[BILIN ? 1 : kGChunk];
-    __shared__ float ssrc[kGChunk][3];
+    __shared__ float ssrc[kGChunk][4];  // source x, y, z, 1 / |(x, y)|
 
     const int64_t nvox = (int64_t)P.n[0] * P.n[1] * P.n[2];
     const int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x;
@@ -112,6 +141,7 @@ __global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPPa
             ssrc[t][0] = sp.source_pos.x;
             ssrc[t][1] = sp.source_pos.y;
             ssrc[t][2] = sp.source_pos.z;
+            ssrc[t][3] = rsqrtf(sp.source_pos.x * sp.source_pos.x + sp.source_pos.y * sp.source_pos.y);
         }
         __syncthreads();
         if (!live) continue;
@@ -128,7 +158,8 @@ __global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPPa
             }
             float s = 0.f, s2 = 0.f;
             for (int t = 0; t < cn; ++t) {
-                const float w = gbc_weight(G.R, wp[0], wp[1], wp[2], ssrc[t][0], ssrc[t][1], ssrc[t][2], G.soft);
+                const float w =
+                    gbc_weight(G.inv_R, wp[0], wp[1], wp[2], ssrc[t][0], ssrc[t][1], ssrc[t][2], ssrc[t][3], G.soft);
                 s2 += w;
                 if (w == 0.f) continue;
                 const ab_bpview &b = sv[t];
@@ -176,23 +207,36 @@ __global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPPa
 // (the first with weight 1/2) and num_ang source angles t in [0, pi) of the
 // weight of the voxel (r, 0, 0) for the source (cos t, sin t, z), times
 // 4 z_max pi / (num_z num_ang) (get_GBC_weight_integ, CB_backproject.cu:1108-1168).
-// One thread per (z, angle) sample; per radius an FP64 block sum and one
-// atomic add.
+// kSPT (height, angle) samples per thread, held in registers across the
+// radii; per radius an FP64 block sum and one atomic add.
+constexpr int kSPT = 8;  // samples per thread of the weight integral
+
 __global__ void __launch_bounds__(kGThreads) k_gbc_weight_integ(const float *r_on_R, int nr, double *out, int num_z,
-                                                                int num_ang, GbcSoft S) {
+                                                                int num_ang, GbcSoft S, float tan_v) {
     __shared__ double warp_sums[kGThreads / 32];
-    const int64_t e = (int64_t)blockIdx.x * kGThreads + threadIdx.x;
-    const bool live = e < (int64_t)num_z * num_ang;
-    const int iz = live ? (int)(e / num_ang) : 0, ia = live ? (int)(e % num_ang) : 0;
-    const float maxz = tanf(S.v) * (1.f + r_on_R[nr - 1]);
-    const float z = maxz * (float)iz / (float)(num_z - 1);
-    const float t = (float)ia / (float)num_ang * 3.1415926535898f;
-    const float sx = cosf(t), sy = sinf(t);
-    const float half = iz == 0 ? 0.5f : 1.f;
+    const int64_t n = (int64_t)num_z * num_ang;
+    const float maxz = tan_v * (1.f + r_on_R[nr - 1]);  // tan(soft_vartheta_v) (1 + r_max)
+    // this thread's samples: source position and end weight (0 past the end)
+    float sx[kSPT], sy[kSPT], sz[kSPT], half[kSPT];
+#pragma unroll
+    for (int k = 0; k < kSPT; ++k) {
+        const int64_t e = ((int64_t)blockIdx.x * kSPT + k) * kGThreads + threadIdx.x;
+        const bool live = e < n;
+        const int iz = live ? (int)(e / num_ang) : 0, ia = live ? (int)(e % num_ang) : 0;
+        sz[k] = maxz * (float)iz / (float)(num_z - 1);
+        const float t = (float)ia / (float)num_ang * 3.1415926535898f;
+        sx[k] = cosf(t);
+        sy[k] = sinf(t);
+        half[k] = !live ? 0.f : (iz == 0 ? 0.5f : 1.f);
+    }
     const double mult = (double)((4.f * maxz * 3.1415926535898f) / ((float)num_z * (float)num_ang));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int r = 0; r < nr; ++r) {
-        double w = live ? (double)(gbc_weight(1.f, r_on_R[r], 0.f, 0.f, sx, sy, z, S) * half) : 0.0;
+        const float rr = r_on_R[r];
+        double w = 0.0;
+#pragma unroll
+        for (int k = 0; k < kSPT; ++k)
+            if (half[k] != 0.f) w += (double)(gbc_weight(1.f, rr, 0.f, 0.f, sx[k], sy[k], sz[k], 1.f, S) * half[k]);
 #pragma unroll
         for (int k = 16; k > 0; k >>= 1) w += __shfl_xor_sync(0xffffffffu, w, k);
         if (lane == 0) warp_sums[warp] = w;
@@ -349,9 +393,9 @@ extern "C" int aprict_b200_backproject_gbc(const aprict_proj_spec *specs_dev, co
     if (rc != APRICT_OK || units == 0) return rc;
     GbcParams G;
     G.vol2 = weightsum_dev;
-    G.R = cfg->Z_on_val_factor_val;
-    G.soft = GbcSoft{cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan, cfg->soft_vartheta_h,
-                     cfg->soft_vartheta_h_softspan};
+    G.inv_R = (float)(1.0 / (double)cfg->Z_on_val_factor_val);
+    G.soft = GbcSoft{soft_win(cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan),
+                     soft_win(cfg->soft_vartheta_h, cfg->soft_vartheta_h_softspan)};
     G.pos000[0] = vd->corner.x + 0.5f * vd->voxwid;
     G.pos000[1] = vd->corner.y + 0.5f * vd->voxwid;
     G.pos000[2] = vd->corner.z + 0.5f * vd->voxwid;
@@ -377,11 +421,13 @@ extern "C" int aprict_b200_gbc_weight_integral(const float *r_on_R_dev, int32_t 
     if (num_z < 2 || num_ang < 1 || (int64_t)num_z * num_ang > (int64_t)1 << 31)
         return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "num_z must be >= 2, num_ang >= 1, num_z * num_ang <= 2^31");
     if (!finite_soft(cfg)) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "non-finite soft windows");
-    const GbcSoft S{cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan, cfg->soft_vartheta_h,
-                    cfg->soft_vartheta_h_softspan};
+    const GbcSoft S{soft_win(cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan),
+                    soft_win(cfg->soft_vartheta_h, cfg->soft_vartheta_h_softspan)};
     const int64_t n = (int64_t)num_z * num_ang;
-    k_gbc_weight_integ<<<(unsigned)((n + kGThreads - 1) / kGThreads), kGThreads, 0,
-                         reinterpret_cast<cudaStream_t>(stream)>>>(r_on_R_dev, n_r, out_dev, num_z, num_ang, S);
+    const int64_t per_block = (int64_t)kGThreads * kSPT;
+    k_gbc_weight_integ<<<(unsigned)((n + per_block - 1) / per_block), kGThreads, 0,
+                         reinterpret_cast<cudaStream_t>(stream)>>>(r_on_R_dev, n_r, out_dev, num_z, num_ang, S,
+                                                              (float)tan((double)cfg->soft_vartheta_v));
     return ab_cuda_check(cudaGetLastError(), "gbc_weight_integral launch");
 }
 
