@@ -41,6 +41,20 @@ class _Config:
     mode: str = "reference"  # "reference" | "classical"
 
 
+class _HostPipeline:
+    """Buffers, streams and events of SIRT_flatpanel.iterate_from_host."""
+
+    def __init__(self, meas: torch.Tensor, vol: torch.Tensor) -> None:
+        self.up, self.down = torch.cuda.Stream(), torch.cuda.Stream()
+        self.b = [torch.empty_like(meas) for _ in range(2)]
+        self.snap = [torch.empty_like(vol) for _ in range(2)]
+        self.uploaded = [torch.cuda.Event() for _ in range(2)]
+        self.consumed = [torch.cuda.Event() for _ in range(2)]
+        self.snapped = [torch.cuda.Event() for _ in range(2)]
+        self.read_back = [torch.cuda.Event() for _ in range(2)]
+        self.k = 0
+
+
 class SIRT_flatpanel:  # noqa: N801
     """An iterable SIRT reconstructor."""
 
@@ -59,6 +73,7 @@ class SIRT_flatpanel:  # noqa: N801
         self._iterations = 0
         self._graph: torch.cuda.CUDAGraph | None = None
         self._graph_n = 0
+        self._pipe: _HostPipeline | None = None
         self._config_fp_residual = fp.ConfigProject(multiply_before_adding=-1)
         sep = 0 if config.bp_soft_from_detedge_relrad is None else (1 - config.bp_soft_from_detedge_relrad)
         cyl = min(*volume.shape[:2]) / 2 * volume.voxwid
@@ -128,6 +143,64 @@ class SIRT_flatpanel:  # noqa: N801
         """Perform one iteration (asynchronous on the current stream)."""
         self._step()
         self._iterations += 1
+
+    def iterate_from_host(self, b_host: torch.Tensor, x_host: torch.Tensor | None = None) -> None:
+        """One iteration whose measurement comes from host memory and whose
+        result goes back to host memory, with both transfers overlapped with
+        the neighbouring iterations' compute (asynchronous on the current stream).
+
+        ``b_host``: this iteration's measurement b, a pinned host tensor of the
+        projection data's shape. It is uploaded on an upload stream into one of
+        two device buffers of this iterator (the ProjectionSet given to
+        ``__init__`` is not touched); the iteration waits only for its own
+        upload, so the next call's upload runs while this iteration computes.
+        ``x_host``: a pinned host tensor of the volume's shape that receives the
+        volume after this iteration: the volume is copied to one of two device
+        snapshots (a device-to-device copy) and read back on a download stream
+        while the next iteration runs. Keep ``b_host`` unchanged and read
+        ``x_host`` only after :meth:`host_sync` (or a device synchronisation).
+        """
+        if tuple(b_host.shape) != tuple(self._meas.data.shape):
+            msg = "b_host must have the projection data's shape"
+            raise ValueError(msg)
+        if x_host is not None and tuple(x_host.shape) != tuple(self._vol.data.shape):
+            msg = "x_host must have the volume's shape"
+            raise ValueError(msg)
+        if self._pipe is None:
+            self._pipe = _HostPipeline(self._meas.data, self._vol.data)
+        pp = self._pipe
+        i = pp.k % 2
+        compute = torch.cuda.current_stream()
+        with torch.cuda.stream(pp.up):
+            pp.up.wait_event(pp.consumed[i])  # the iteration that read buffer i two calls ago is done with it
+            pp.b[i].copy_(b_host, non_blocking=True)
+            pp.b[i].record_stream(pp.up)
+            pp.uploaded[i].record(pp.up)
+        compute.wait_event(pp.uploaded[i])
+        fp.project_residual(self._config_fp_residual, self._vol, self._scratch, pp.b[i])
+        pp.consumed[i].record(compute)
+        if self._rownorm is not None:
+            self._scratch.data.mul_(self._rownorm)
+        fp.backproject(self._config_bp, self._vol, self._scratch, summand_multiplier=self._precond)
+        if x_host is not None:
+            compute.wait_event(pp.read_back[i])  # snapshot i's previous read-back has ended
+            pp.snap[i].copy_(self._vol.data)
+            pp.snapped[i].record(compute)
+            with torch.cuda.stream(pp.down):
+                pp.down.wait_event(pp.snapped[i])
+                x_host.copy_(pp.snap[i], non_blocking=True)
+                pp.snap[i].record_stream(pp.down)
+                pp.read_back[i].record(pp.down)
+        pp.k += 1
+        self._iterations += 1
+
+    def host_sync(self) -> None:
+        """Make the current stream wait for every transfer of :meth:`iterate_from_host` and block until done."""
+        if self._pipe is not None:
+            s = torch.cuda.current_stream()
+            s.wait_stream(self._pipe.up)
+            s.wait_stream(self._pipe.down)
+        torch.cuda.current_stream().synchronize()
 
     def iterate_graph(self, n: int) -> None:
         """Perform ``n`` iterations by replaying one captured CUDA graph.

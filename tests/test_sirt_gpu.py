@@ -102,6 +102,31 @@ def test_graph_replay_equals_eager() -> None:
     assert rel_l2(xb.as_numpy(), xa.as_numpy()) <= 1e-6
 
 
+def test_iterate_from_host_equals_eager() -> None:
+    # a different measurement every step (as a stream of scans would give) and the
+    # volume read back after each: the pipelined transfers change no result
+    pg, _, b = _problem()
+    xa = Volume.zeros(SHAPE, voxwid=1.0)
+    xb = Volume.zeros(SHAPE, voxwid=1.0)
+    sa = SIRT_flatpanel(SIRT_flatpanel.Config(), xa, fp.ProjectionSet(pg, data=b.clone()))
+    sb = SIRT_flatpanel(SIRT_flatpanel.Config(), xb, fp.ProjectionSet(pg, data=b.clone()))
+    bs = [(b * (1.0 + 0.1 * k)).cpu().pin_memory() for k in range(5)]
+    outs = [torch.empty(SHAPE, dtype=torch.float32).pin_memory() for _ in range(5)]
+    want = []
+    for k in range(5):
+        sa._meas.data.copy_(bs[k])  # noqa: SLF001
+        sa.iterate()
+        want.append(xa.as_numpy().copy())
+    for k in range(5):
+        sb.iterate_from_host(bs[k], outs[k])
+    sb.host_sync()
+    assert sb.iterations == 5
+    for k in range(5):
+        assert rel_l2(outs[k].numpy(), want[k]) <= 1e-6
+    assert np.abs(want[4] - want[3]).max() > 0
+    assert torch.equal(sb._meas.data, b)  # noqa: SLF001  the caller's ProjectionSet is untouched
+
+
 def test_sirt_converges_and_checkpoints(tmp_path) -> None:
     pg, xt, b = _problem()
     x = Volume.zeros(SHAPE, voxwid=1.0)
