@@ -84,6 +84,9 @@ def _scan_record(volume: Volume, projs: fp.ProjectionSet) -> np.ndarray:
     if not volume.data.is_cuda:
         msg = "Volume data must live on the GPU."
         raise ValueError(msg)
+    if volume.data.dtype != torch.float32 or projs.data.dtype != torch.float32:
+        msg = "batched scans take float32 volumes and projections (one-scan calls take float16 / float64 too)"
+        raise NotImplementedError(msg)
     rec = np.zeros((), S.scan)
     d = projs.data
     rec["specs_dev"] = projs.specs_device().data_ptr()
@@ -139,8 +142,8 @@ class ScanBatch:
                 raise ValueError(msg)
             for i, b in enumerate(bases):
                 d = self.projs[i].data
-                if tuple(b.shape) != tuple(d.shape) or b.stride() != d.stride() or not b.is_cuda:
-                    msg = "each base must be a CUDA tensor with the shape and strides of its projection data"
+                if tuple(b.shape) != tuple(d.shape) or b.stride() != d.stride() or not b.is_cuda or b.dtype != torch.float32:
+                    msg = "each base must be a float32 CUDA tensor with the shape and strides of its projection data"
                     raise ValueError(msg)
                 recs[i]["base_dev"] = b.data_ptr()
             keep += list(bases)

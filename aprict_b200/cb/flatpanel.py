@@ -5,7 +5,8 @@ src/aprict/cb/flatpanel.py:
   * ``ProjGeom`` (:269-768): per-view source, detector centre and pixel vectors,
     regularised to float32 on construction (:311-318, :612-622);
   * ``ProjectionSet`` (:771-882): a geometry plus a (..., M, nu, nv) float32
-    device array (a torch tensor here, v fastest);
+    (or float16 / float64, as the reference allows) device array (a torch
+    tensor here, v fastest);
   * ``ConfigProject`` / ``ConfigBackproject`` (:885-994);
   * ``project`` (:997-1125) and ``backproject`` (:1128-1281), which ADD into
     their output.
@@ -344,18 +345,28 @@ class ProjGeom:
 
 
 # --------------------------------------------------------------------------- data
+# Projection data types of the reference's kernels (half, float, double; flatpanel.py:120-185).
+# The kernels here compute in FP32: other types pass through FP32 working copies.
+_PROJ_DTYPES = {np.dtype(np.float16): torch.float16, np.dtype(np.float32): torch.float32,
+                np.dtype(np.float64): torch.float64}
+
+
+def _np_dtype(t: torch.Tensor) -> np.dtype:
+    return np.dtype(str(t.dtype).replace("torch.", ""))
+
+
 class ProjectionSet:
     """A projection geometry with (optionally) its detector data on the GPU."""
 
     def __init__(self, pg: ProjGeom, *, data: np.ndarray | torch.Tensor | None) -> None:
         if data is not None:
             if isinstance(data, np.ndarray):
-                if data.dtype != np.float32:
-                    msg = f"Projection dtype {data.dtype} is not supported (float32 only)."
+                if data.dtype not in _PROJ_DTYPES:
+                    msg = f"Projection dtype {data.dtype} is not supported (float16, float32 or float64)."
                     raise NotImplementedError(msg)
                 data = torch.from_numpy(np.ascontiguousarray(data)).to(_device())
-            elif data.dtype != torch.float32:
-                msg = f"Projection dtype {data.dtype} is not supported (float32 only)."
+            elif data.dtype not in _PROJ_DTYPES.values():
+                msg = f"Projection dtype {data.dtype} is not supported (float16, float32 or float64)."
                 raise NotImplementedError(msg)
             elif not data.is_cuda:
                 data = data.to(_device())
@@ -412,11 +423,11 @@ class ProjectionSet:
                 return
             msg = "Data buffer already exists. Pass 'existing_ok=True' to allow this to occur without raising an exception."
             raise RuntimeError(msg)
-        if np.dtype(dtype) != np.float32:
-            msg = f"Projection dtype {np.dtype(dtype)} is not supported (float32 only)."
+        if np.dtype(dtype) not in _PROJ_DTYPES:
+            msg = f"Projection dtype {np.dtype(dtype)} is not supported (float16, float32 or float64)."
             raise NotImplementedError(msg)
         shape = _assert_flatpanel_geometry_consistency(self._proj_specs, None)
-        self._data = torch.zeros(shape, dtype=torch.float32, device=_device())
+        self._data = torch.zeros(shape, dtype=_PROJ_DTYPES[np.dtype(dtype)], device=_device())
 
     def zeroed_copy(self, dtype: type | np.dtype | None = None) -> ProjectionSet:
         """A copy with a zero-filled buffer."""
@@ -425,7 +436,7 @@ class ProjectionSet:
             raise ValueError(msg)
         ps = ProjectionSet(self._proj_geom, data=None)
         ps._specs_dev = self._specs_dev
-        ps.create_buffer(dtype=np.float32 if dtype is None else dtype)
+        ps.create_buffer(dtype=_np_dtype(self._data) if dtype is None else dtype)
         return ps
 
 
@@ -533,14 +544,40 @@ def _leading_slices(projs: ProjectionSet) -> list[tuple[tuple[int, ...], int]]:
     return [(it, int(np.ravel_multi_index(it, lead)) * m if lead else 0) for it in itertools.product(*map(range, lead))]
 
 
-def _view_args(projs: ProjectionSet, it: tuple[int, ...], first: int) -> tuple[int, np.ndarray, int]:
-    data = projs.data
+def _view_args(projs: ProjectionSet, it: tuple[int, ...], first: int,
+               data: torch.Tensor | None = None) -> tuple[int, np.ndarray, int]:
+    data = projs.data if data is None else data
     assert data is not None
     sub = data[it] if it else data
     m, nu, nv = sub.shape[-3:]
     pd = _lib.proj_desc((m, nu, nv), tuple(sub.stride()[-3:]))
     specs = projs.specs_device().data_ptr() + first * S.proj_spec.itemsize
     return specs, pd, sub.data_ptr()
+
+
+def _f32_twin(projs: ProjectionSet) -> ProjectionSet:
+    """``projs`` itself when its data is float32, else a zero-filled float32
+    twin with the same geometry (and overflow counter) for the kernels to add
+    into; :func:`_fold_twin` adds it back."""
+    assert projs.data is not None
+    if projs.data.dtype == torch.float32:
+        return projs
+    tw = ProjectionSet(projs.proj_geom, data=torch.zeros(projs.data.shape, dtype=torch.float32, device=projs.data.device))
+    tw._specs_dev = projs._specs_dev  # noqa: SLF001
+    tw._out_of_mem_counter = projs.out_of_mem_counter  # noqa: SLF001
+    return tw
+
+
+def _fold_twin(projs: ProjectionSet, tw: ProjectionSet) -> None:
+    """projs.data += tw.data in projs' own dtype (exact for float64, one rounding for float16)."""
+    if tw is not projs:
+        assert projs.data is not None and tw.data is not None
+        projs.data.add_(tw.data.to(projs.data.dtype) if projs.data.dtype == torch.float64 else tw.data)
+
+
+def _f32_data(t: torch.Tensor) -> torch.Tensor:
+    """A float32 tensor with t's values and strides: t itself, or a converted copy."""
+    return t if t.dtype == torch.float32 else t.float()
 
 
 def _check_volume_device(volume: Volume) -> None:
@@ -557,25 +594,28 @@ def project(
 ) -> ProjectionSet:
     """Add the projection of ``volume`` into ``projs`` (flatpanel.py:997-1125)."""
     projs.create_buffer(dtype=np.float32, existing_ok=True)
+    work = _f32_twin(projs)  # float16 / float64 data: project into float32, then add
     if type(volume) is FBVolume:
         from . import forbild  # noqa: PLC0415
 
-        forbild.project_shapes(config, volume, projs)
+        forbild.project_shapes(config, volume, work)
     elif type(volume) is Volume:
         _check_volume_device(volume)
         cfg = config.contents
         vd = volume._desc()  # noqa: SLF001
-        for it, first in _leading_slices(projs):
-            specs, pd, dptr = _view_args(projs, it, first)
+        v32 = volume._f32()  # noqa: SLF001
+        for it, first in _leading_slices(work):
+            specs, pd, dptr = _view_args(work, it, first)
             _lib.check(
                 _lib.lib().aprict_b200_project_siddon(
-                    specs, _lib.ptr(pd), dptr, None, _lib.ptr(vd), volume.data.data_ptr(), _lib.ptr(cfg), None, _stream()
+                    specs, _lib.ptr(pd), dptr, None, _lib.ptr(vd), v32.data_ptr(), _lib.ptr(cfg), None, _stream()
                 ),
                 "project",
             )
     else:
         msg = f"Unknown volume type: {type(volume)}"
         raise RuntimeError(msg)
+    _fold_twin(projs, work)
     if block:
         torch.cuda.current_stream().synchronize()
     return projs
@@ -594,15 +634,19 @@ def project_residual(config: ConfigProject, volume: Volume, projs: ProjectionSet
         raise ValueError(msg)
     cfg = config.contents
     vd = volume._desc()  # noqa: SLF001
+    v32, b32 = volume._f32(), _f32_data(base)  # noqa: SLF001
+    out = _f32_data(projs.data)
     for it, first in _leading_slices(projs):
-        specs, pd, dptr = _view_args(projs, it, first)
-        bsub = base[it] if it else base
+        specs, pd, dptr = _view_args(projs, it, first, data=out)
+        bsub = b32[it] if it else b32
         _lib.check(
             _lib.lib().aprict_b200_project_siddon(
-                specs, _lib.ptr(pd), dptr, bsub.data_ptr(), _lib.ptr(vd), volume.data.data_ptr(), _lib.ptr(cfg), None, _stream()
+                specs, _lib.ptr(pd), dptr, bsub.data_ptr(), _lib.ptr(vd), v32.data_ptr(), _lib.ptr(cfg), None, _stream()
             ),
             "project_residual",
         )
+    if out is not projs.data:
+        projs.data.copy_(out)
     return projs
 
 
@@ -637,7 +681,11 @@ def backproject(
         raise NotImplementedError(msg)
     _check_volume_device(volume)
     vd = volume._desc()  # noqa: SLF001
-    mptr = summand_multiplier.data.data_ptr() if summand_multiplier is not None else None
+    # FP32 working copies of float16 volumes / non-FP32 projections (the kernels compute in FP32)
+    v32 = volume._f32()  # noqa: SLF001
+    m32 = summand_multiplier._f32() if summand_multiplier is not None else None  # noqa: SLF001
+    mptr = m32.data_ptr() if m32 is not None else None
+    p32 = _f32_data(projs.data)
     if preset == 7:
         # the GBC kernel, with the weight sums in the secondary volume (flatpanel.py:216-232)
         if secondary_volume is None:
@@ -647,26 +695,30 @@ def backproject(
             msg = "The secondary volume must have the volume's shape and memory order."
             raise ValueError(msg)
         _check_volume_device(secondary_volume)
+        s32 = secondary_volume._f32()  # noqa: SLF001
         for it, first in _leading_slices(projs):
-            specs, pd, dptr = _view_args(projs, it, first)
+            specs, pd, dptr = _view_args(projs, it, first, data=p32)
             _lib.check(
                 _lib.lib().aprict_b200_backproject_gbc(
-                    specs, _lib.ptr(pd), dptr, _lib.ptr(vd), volume.data.data_ptr(), secondary_volume.data.data_ptr(),
+                    specs, _lib.ptr(pd), dptr, _lib.ptr(vd), v32.data_ptr(), s32.data_ptr(),
                     mptr, _lib.ptr(cfg), None, _stream(),
                 ),
                 "backproject_gbc",
             )
+        volume._commit(v32)  # noqa: SLF001
+        secondary_volume._commit(s32)  # noqa: SLF001
         if block:
             torch.cuda.current_stream().synchronize()
         return volume
     for it, first in _leading_slices(projs):
-        specs, pd, dptr = _view_args(projs, it, first)
+        specs, pd, dptr = _view_args(projs, it, first, data=p32)
         _lib.check(
             _lib.lib().aprict_b200_backproject(
-                specs, _lib.ptr(pd), dptr, _lib.ptr(vd), volume.data.data_ptr(), mptr, _lib.ptr(cfg), None, _stream()
+                specs, _lib.ptr(pd), dptr, _lib.ptr(vd), v32.data_ptr(), mptr, _lib.ptr(cfg), None, _stream()
             ),
             "backproject",
         )
+    volume._commit(v32)  # noqa: SLF001
     if block:
         torch.cuda.current_stream().synchronize()
     return volume
@@ -686,14 +738,16 @@ def backproject_adjoint(
     _check_volume_device(volume)
     cfg = config.contents
     vd = volume._desc()  # noqa: SLF001
+    v32, p32 = volume._f32(), _f32_data(projs.data)  # noqa: SLF001
     for it, first in _leading_slices(projs):
-        specs, pd, dptr = _view_args(projs, it, first)
+        specs, pd, dptr = _view_args(projs, it, first, data=p32)
         _lib.check(
             _lib.lib().aprict_b200_backproject_scatter(
-                specs, _lib.ptr(pd), dptr, _lib.ptr(vd), volume.data.data_ptr(), _lib.ptr(cfg), None, _stream()
+                specs, _lib.ptr(pd), dptr, _lib.ptr(vd), v32.data_ptr(), _lib.ptr(cfg), None, _stream()
             ),
             "backproject_adjoint",
         )
+    volume._commit(v32)  # noqa: SLF001
     if block:
         torch.cuda.current_stream().synchronize()
     return volume

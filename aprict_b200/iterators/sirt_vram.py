@@ -77,7 +77,7 @@ class SIRT_flatpanel:  # noqa: N801
         self._config_fp_residual = fp.ConfigProject(multiply_before_adding=-1)
         sep = 0 if config.bp_soft_from_detedge_relrad is None else (1 - config.bp_soft_from_detedge_relrad)
         cyl = min(*volume.shape[:2]) / 2 * volume.voxwid
-        p = projs.zeroed_copy()
+        p = projs.zeroed_copy(dtype=np.float32)  # the residual is FP32 whatever the measurement's type
         if config.mode == "reference":
             self._config_bp = fp.ConfigBackproject(
                 fast_approx=config.fast_backproject,

@@ -89,7 +89,7 @@ def fbp_fan_circ(
     filt = FBPFilterer(L=L, physpixwid=pixwid, proj_2d_shape=(nu, nv), _hacky_fan_beam_mode=True, apodization=apodization)
     scale = 1.0 / (4.0 * np.pi * R * m)
     outs = None if filtered_out is None else [filtered_out]
-    (filtered,) = filt.rfilt.filter(projs.data, weights=filt._weights, scale=scale, outs=outs)  # noqa: SLF001
+    (filtered,) = filt.rfilt.filter(projs.data.float(), weights=filt._weights, scale=scale, outs=outs)  # noqa: SLF001
     support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
     cfg = fp.ConfigBackproject(
         fast_approx=True,
@@ -133,7 +133,7 @@ def fbp_fan_circ_batch(
         raise NotImplementedError(msg)
     R, L, pixwid, nu, nv = geo[0]  # noqa: N806
     if stacked is None:
-        stacked = torch.cat([p.data for p in projs], dim=0)
+        stacked = torch.cat([p.data.float() for p in projs], dim=0)
     filt = FBPFilterer(L=L, physpixwid=pixwid, proj_2d_shape=(nu, nv), _hacky_fan_beam_mode=True, apodization=apodization)
     (filtered,) = filt.rfilt.filter(stacked, weights=filt._weights, scale=1.0 / (4.0 * np.pi * R * m))  # noqa: SLF001
     support = R * np.sin(np.arctan(pixwid * nu / 2 / L))
@@ -213,7 +213,7 @@ def fbp_cone_cyl(
         if z1 < src_z[sl].min() - hdiff or z0 > src_z[sl].max() + hdiff:
             filt.advance_rng(sl.stop - sl.start)  # out of reach of the volume
             continue
-        chunk = data[sl]
+        chunk = data[sl].float()
         if angs is None:
             outs, _ = filt.filter_bulk_axis1_concat(chunk, force_rotation_angle=None, block=False)
         else:

@@ -3,8 +3,11 @@
 Mirrors ``aprict.volume`` (src/aprict/volume/volume.py:51-495). The reference
 stores a ``Volume`` in a CUDA array behind a surface object; users never touch
 the texture (src/aprict/volume/volume.py:18-20), so here the storage is a
-linear float32 device buffer (a torch tensor with C- or F-order strides) that
-the kernels index directly. Voxel centres follow the reference convention:
+linear device buffer (a torch tensor with C- or F-order strides) that the
+kernels index directly: float32, or float16 as the reference also allows
+(:44-45). The kernels compute in FP32; a float16 volume is read through an
+FP32 working copy and written back rounded (element-wise operations, the
+projector and the backprojector alike). Voxel centres follow the reference convention:
 ``pos_c + voxwid * (i - (n-1)/2)`` (volume.py:133-145).
 """
 
@@ -20,7 +23,8 @@ import torch
 
 from . import _lib
 
-_SUPPORTED_DTYPES = (np.dtype(np.float32),)
+_SUPPORTED_DTYPES = (np.dtype(np.float32), np.dtype(np.float16))
+_TORCH_DTYPES = {np.dtype(np.float32): torch.float32, np.dtype(np.float16): torch.float16}
 
 
 def _stream() -> int:
@@ -34,10 +38,10 @@ def _device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
-def _empty(shape: tuple[int, int, int], order: str) -> torch.Tensor:
+def _empty(shape: tuple[int, int, int], order: str, dtype: torch.dtype = torch.float32) -> torch.Tensor:
     X, Y, Z = shape
     strides = (Y * Z, Z, 1) if order == "C" else (1, X, X * Y)
-    return torch.empty_strided(shape, strides, dtype=torch.float32, device=_device())
+    return torch.empty_strided(shape, strides, dtype=dtype, device=_device())
 
 
 class Volume:
@@ -67,7 +71,7 @@ class Volume:
             raise ValueError(msg)
         dt = np.dtype(str(arr.dtype).replace("torch.", ""))
         if dt not in _SUPPORTED_DTYPES:
-            msg = f"Volume dtype {dt} is not supported (float32 only)."
+            msg = f"Volume dtype {dt} is not supported (float32 or float16)."
             raise NotImplementedError(msg)
         self._dtype = dt
         self._shape = tuple(int(s) for s in arr.shape)  # type: ignore[assignment]
@@ -75,7 +79,7 @@ class Volume:
         self._voxwid = float(voxwid)
         self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
         if initialize_texture:
-            self._data = _empty(self._shape, order)
+            self._data = _empty(self._shape, order, _TORCH_DTYPES[dt])
             self.copy_from(arr)
 
     # ------------------------------------------------------------------ props
@@ -142,6 +146,15 @@ class Volume:
     def _desc(self) -> np.ndarray:
         return _lib.vol_desc(self._shape, self._order, self._voxwid, self.corner)
 
+    def _f32(self) -> torch.Tensor:
+        """The data as float32 with the same strides: the tensor itself, or a copy of a float16 volume."""
+        return self._data if self._data.dtype == torch.float32 else self._data.float()
+
+    def _commit(self, t: torch.Tensor) -> None:
+        """Store a float32 working copy from :meth:`_f32` back (a no-op when it is the data itself)."""
+        if t is not self._data:
+            self._data.copy_(t)
+
     @property
     def _numel(self) -> int:
         return int(np.prod(self._shape))
@@ -149,36 +162,42 @@ class Volume:
     # --------------------------------------------------------------- elementwise
     def fill(self, value: float) -> None:
         """Fill the volume with a constant value."""
+        w = self._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_fill(self._data.data_ptr(), self._numel, float(value), _stream()),
+            _lib.lib().aprict_b200_vol_fill(w.data_ptr(), self._numel, float(value), _stream()),
             "Volume.fill",
         )
+        self._commit(w)
 
     def multiply(self, f: float) -> None:
         """Multiply the volume in place by a value."""
+        w = self._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_scale(self._data.data_ptr(), self._numel, float(f), _stream()),
+            _lib.lib().aprict_b200_vol_scale(w.data_ptr(), self._numel, float(f), _stream()),
             "Volume.multiply",
         )
+        self._commit(w)
 
     def invert(self, *, ignore_zeros: bool = False, softmax_epsilon: float | None = None) -> None:
         """v <- 1/(v + eps exp(-v/eps)) (texture_tools.operations.invert, operations.py:347-374)."""
+        w = self._f32()
         _lib.check(
             _lib.lib().aprict_b200_vol_invert(
-                self._data.data_ptr(), self._numel, int(bool(ignore_zeros)), float(softmax_epsilon or 0), _stream()
+                w.data_ptr(), self._numel, int(bool(ignore_zeros)), float(softmax_epsilon or 0), _stream()
             ),
             "Volume.invert",
         )
+        self._commit(w)
 
     def multiply_volume(self, other: Volume) -> None:
         """Element-wise product with another volume of the same shape and order."""
         self._check_same(other)
+        w, o = self._f32(), other._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_mul(
-                self._data.data_ptr(), self._data.data_ptr(), other._data.data_ptr(), self._numel, _stream()
-            ),
+            _lib.lib().aprict_b200_vol_mul(w.data_ptr(), w.data_ptr(), o.data_ptr(), self._numel, _stream()),
             "Volume.multiply_volume",
         )
+        self._commit(w)
 
     def divide(self, other: Volume) -> None:
         """Element-wise division by another volume (divide_textures)."""
@@ -188,12 +207,14 @@ class Volume:
         """self <- self / (other + eps exp(-other / eps)) (volume.py:196-200,
         divide_surfaces_softzero); eps <= 0 divides plainly."""
         self._check_same(other)
+        w, o = self._f32(), other._f32()
         _lib.check(
             _lib.lib().aprict_b200_vol_div_softzero(
-                self._data.data_ptr(), self._data.data_ptr(), other._data.data_ptr(), self._numel, float(eps), _stream()
+                w.data_ptr(), w.data_ptr(), o.data_ptr(), self._numel, float(eps), _stream()
             ),
             "Volume.divide_softzero",
         )
+        self._commit(w)
 
     def multiply_by_xygrid(self, xygrid: np.ndarray | torch.Tensor) -> None:
         """Multiply in place by an (nx, ny) grid broadcast over z (volume.py:170-190)."""
@@ -202,34 +223,30 @@ class Volume:
             msg = "Input array should be 2-dimensional and match the shape[:2] of this volume."
             raise ValueError(msg)
         vd = self._desc()
+        w = self._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_mul_xygrid(self._data.data_ptr(), _lib.ptr(vd), g.data_ptr(), _stream()),
+            _lib.lib().aprict_b200_vol_mul_xygrid(w.data_ptr(), _lib.ptr(vd), g.data_ptr(), _stream()),
             "Volume.multiply_by_xygrid",
         )
+        self._commit(w)
 
     def add_scaled(self, other: Volume, alpha: float) -> None:
         """self += alpha * other."""
         self._check_same(other)
+        w, o = self._f32(), other._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_axpy(
-                self._data.data_ptr(),
-                self._data.data_ptr(),
-                float(alpha),
-                other._data.data_ptr(),
-                self._numel,
-                _stream(),
-            ),
+            _lib.lib().aprict_b200_vol_axpy(w.data_ptr(), w.data_ptr(), float(alpha), o.data_ptr(), self._numel, _stream()),
             "Volume.add_scaled",
         )
+        self._commit(w)
 
     def inner_product(self, other: Volume) -> float:
         """<self, other> accumulated in double on the device."""
         self._check_same(other)
         out = torch.zeros((), dtype=torch.float64, device=self._data.device)
+        a, b = self._f32(), other._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_dot(
-                self._data.data_ptr(), other._data.data_ptr(), self._numel, out.data_ptr(), _stream()
-            ),
+            _lib.lib().aprict_b200_vol_dot(a.data_ptr(), b.data_ptr(), self._numel, out.data_ptr(), _stream()),
             "Volume.inner_product",
         )
         return float(out.item())
@@ -240,12 +257,12 @@ class Volume:
             msg = "The input 'relrad_start' should be between 0 and 1."
             raise ValueError(msg)
         d = self._desc()
+        w = self._f32()
         _lib.check(
-            _lib.lib().aprict_b200_vol_softmask_cylinder(
-                self._data.data_ptr(), _lib.ptr(d), float(relrad_start), _stream()
-            ),
+            _lib.lib().aprict_b200_vol_softmask_cylinder(w.data_ptr(), _lib.ptr(d), float(relrad_start), _stream()),
             "Volume.soften_to_xy_cylinder",
         )
+        self._commit(w)
 
     def _check_same(self, other: Volume) -> None:
         if other.shape != self.shape:
@@ -262,7 +279,7 @@ class Volume:
             msg = f"Shape mismatch: expected {self._shape}, got {tuple(arr.shape)}"
             raise ValueError(msg)
         src = arr if isinstance(arr, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32))
-        self._data.copy_(src.to(torch.float32), non_blocking=not block)
+        self._data.copy_(src.to(self._data.dtype), non_blocking=not block)
         if block:
             torch.cuda.current_stream().synchronize()
 
@@ -317,7 +334,7 @@ class Volume:
             msg = "Invalid shape provided. It should be a tuple of three positive integers."
             raise ValueError(msg)
         if np.dtype(dtype) not in _SUPPORTED_DTYPES:
-            msg = f"Volume dtype {np.dtype(dtype)} is not supported (float32 only)."
+            msg = f"Volume dtype {np.dtype(dtype)} is not supported (float32 or float16)."
             raise NotImplementedError(msg)
         self = cls.__new__(cls)
         self._shape = tuple(int(s) for s in shape)  # type: ignore[assignment]
@@ -326,8 +343,8 @@ class Volume:
         self._voxwid = float(voxwid)
         self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
         if initialize_texture:
-            self._data = _empty(self._shape, order)
-            self.fill(0.0)
+            self._data = _empty(self._shape, order, _TORCH_DTYPES[self._dtype])
+            self._data.zero_()
         return self
 
     @classmethod
@@ -338,9 +355,9 @@ class Volume:
         voxwid: float,
         pos_c: np.ndarray | tuple[float, float, float] = (0.0, 0.0, 0.0),
     ) -> Volume:
-        """Wrap a float32 CUDA tensor of shape (X,Y,Z) without copying (C- or F-contiguous)."""
-        if t.dim() != 3 or t.dtype != torch.float32 or not t.is_cuda:
-            msg = "from_tensor needs a 3-D float32 CUDA tensor"
+        """Wrap a float32 or float16 CUDA tensor of shape (X,Y,Z) without copying (C- or F-contiguous)."""
+        if t.dim() != 3 or t.dtype not in (torch.float32, torch.float16) or not t.is_cuda:
+            msg = "from_tensor needs a 3-D float32 or float16 CUDA tensor"
             raise ValueError(msg)
         X, Y, Z = t.shape  # noqa: N806
         if t.stride() == (Y * Z, Z, 1):
@@ -352,7 +369,7 @@ class Volume:
             raise ValueError(msg)
         self = cls.__new__(cls)
         self._shape = (int(X), int(Y), int(Z))
-        self._dtype = np.dtype(np.float32)
+        self._dtype = np.dtype(np.float32 if t.dtype == torch.float32 else np.float16)
         self._order = order  # type: ignore[assignment]
         self._voxwid = float(voxwid)
         self._pos_c = np.array(pos_c, dtype=np.float32).reshape(3)
@@ -487,8 +504,10 @@ class FBVolume:
         """Add the phantom, point-sampled at ``volume``'s voxel centres (with
         ``supersamp_factor``^3 sub-samples per voxel), into ``volume``."""
         xs, ys, zs = volume.xs_ys_zs
-        self.to_tensor(xs, ys, zs, out=volume.data, supersamp_cubic_vox_wid=volume.voxwid,
+        w = volume._f32()  # noqa: SLF001
+        self.to_tensor(xs, ys, zs, out=w, supersamp_cubic_vox_wid=volume.voxwid,
                        supersamp_factor=supersamp_factor, block=False)
+        volume._commit(w)  # noqa: SLF001
         return volume
 
     # -------------------------------------------------------- transforms
