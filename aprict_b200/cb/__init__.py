@@ -1,5 +1,7 @@
 """Cone-beam operators (drop-in for ``aprict.cb``)."""
 
-from . import flatpanel
+from . import flatpanel, noop_filter, ramp_filter
+from .noop_filter import NoOpFilterer
+from .ramp_filter import FBPFilterer, RampFilterer
 
-__all__ = ["flatpanel"]
+__all__ = ["FBPFilterer", "NoOpFilterer", "RampFilterer", "flatpanel", "noop_filter", "ramp_filter"]

@@ -405,6 +405,11 @@ class ProjectionSet:
         return self._out_of_mem_counter
 
     @property
+    def out_of_mem_counter_cp(self) -> torch.Tensor:
+        """The overflow counter under the reference's name (a (1,) device array; a torch tensor here)."""
+        return self.out_of_mem_counter
+
+    @property
     def out_of_mem_count(self) -> int:
         """Number of overflowed rays (flatpanel.py:817-820)."""
         return int(self.out_of_mem_counter.item())

@@ -115,6 +115,28 @@ class RampFilterer:
             )
         return outs
 
+    def filter_bulk_axis1_stream(self, arr: torch.Tensor, block: bool = True):  # noqa: ANN201
+        """Generator of (filtered chunks, one per filter; completion event) over chunks of
+        ``projs_per_batch`` projections (ramp_filter.py:242-259)."""
+        per = self.chunk_shape[0]
+        for i in range(0, arr.shape[0], per):
+            outs = self.filter(arr[i : i + per])
+            ev = torch.cuda.Event()
+            ev.record()
+            if block:
+                ev.synchronize()
+            yield outs, ev
+
+    def filter_bulk_axis1_concat(self, arr: torch.Tensor, block: bool = True) -> tuple[list[torch.Tensor], torch.cuda.Event]:
+        """All projections filtered at once: (one (M, nu, nv) array per filter, completion event)
+        (ramp_filter.py:261-305; the convolution kernel takes any number of views per launch)."""
+        outs = self.filter(arr)
+        ev = torch.cuda.Event()
+        ev.record()
+        if block:
+            ev.synchronize()
+        return outs, ev
+
 
 def frame_weight_mask(frame_shape: tuple[int, int], physpixwid: float, L: float, fdk: bool) -> np.ndarray:  # noqa: N803
     """FP64 weights over the padded frame, computed from the reference's float32

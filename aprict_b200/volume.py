@@ -38,6 +38,19 @@ def _device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
+def _to_cupy(t: torch.Tensor) -> object:
+    try:
+        import cupy as cp  # noqa: PLC0415
+    except ImportError as e:
+        msg = "this method returns CuPy arrays and needs CuPy; the torch-returning method beside it does not"
+        raise ImportError(msg) from e
+    return cp.from_dlpack(t)
+
+
+def _from_cupy(a: object) -> torch.Tensor:
+    return torch.from_dlpack(a)
+
+
 def _empty(shape: tuple[int, int, int], order: str, dtype: torch.dtype = torch.float32) -> torch.Tensor:
     X, Y, Z = shape
     strides = (Y * Z, Z, 1) if order == "C" else (1, X, X * Y)
@@ -313,6 +326,54 @@ class Volume:
             raise ImportError(msg) from e
         return cp.from_dlpack(self._data)
 
+    def slice_axis(self, axis: int, sl: slice, *, out: torch.Tensor | None = None) -> torch.Tensor:
+        """A C-contiguous device copy of the voxels ``sl`` along ``axis`` (3-D, this volume's dtype;
+        slice_nth_axis_to_3d_cupy_array, operations.py:404-488)."""
+        if sl.step not in (None, 1):
+            msg = "Cannot use this method with a step size other than 1."
+            raise NotImplementedError(msg)
+        if axis not in (0, 1, 2):
+            msg = "Invalid choice of axis. Choose 0, 1 or 2."
+            raise ValueError(msg)
+        start = 0 if sl.start is None else sl.start
+        stop = self._shape[axis] if sl.stop is None else min(sl.stop, self._shape[axis])
+        if stop - start <= 0:
+            msg = f"Slice is empty. Provided slice: {sl}. Array shape: {self._shape}"
+            raise ValueError(msg)
+        idx = [slice(None)] * 3
+        idx[axis] = slice(start, stop)
+        src = self._data[tuple(idx)]
+        if out is None:
+            return src.contiguous() if not src.is_contiguous() else src.clone()
+        if tuple(out.shape) != tuple(src.shape) or out.dtype != src.dtype or not out.is_contiguous():
+            msg = f"Output must be a C-contiguous {src.dtype} tensor of shape {tuple(src.shape)}."
+            raise ValueError(msg)
+        out.copy_(src)
+        return out
+
+    def sum_axis(self, axis: int, *, out: torch.Tensor | None = None) -> torch.Tensor:
+        """The volume summed along ``axis`` into a 2-D device tensor of this volume's dtype
+        (accumulated in FP64; sum_along_nth_axis_to_2d_cupy_array, operations.py:491-560)."""
+        if axis not in (0, 1, 2):
+            msg = "Invalid choice of axis. Choose 0, 1 or 2."
+            raise ValueError(msg)
+        s = self._data.sum(dim=axis, dtype=torch.float64).to(self._data.dtype)
+        if out is None:
+            return s.contiguous()
+        if tuple(out.shape) != tuple(s.shape) or out.dtype != s.dtype:
+            msg = f"Output must be a {s.dtype} tensor of shape {tuple(s.shape)}."
+            raise ValueError(msg)
+        out.copy_(s)
+        return out
+
+    def as_cupy_slice(self, axis: int, sl: slice, *, out: object | None = None) -> object:
+        """:meth:`slice_axis` as a CuPy array (requires CuPy; zero-copy through DLPack)."""
+        return _to_cupy(self.slice_axis(axis, sl, out=None if out is None else _from_cupy(out)))
+
+    def sum_to_cupy_array(self, axis: int, *, out: object | None = None) -> object:
+        """:meth:`sum_axis` as a CuPy array (requires CuPy; zero-copy through DLPack)."""
+        return _to_cupy(self.sum_axis(axis, out=None if out is None else _from_cupy(out)))
+
     def save(self, path: pathlib.Path | str) -> None:
         """Save the volume to a .npy file."""
         np.save(path, self.as_numpy())
@@ -499,6 +560,12 @@ class FBVolume:
     def to_numpy(self, xs: np.ndarray, ys: np.ndarray, zs: np.ndarray, **kw) -> np.ndarray:
         """:meth:`to_tensor` copied to the host (volume.py:503-508)."""
         return self.to_tensor(xs, ys, zs, **kw).cpu().numpy()
+
+    def to_cupy(self, xs: np.ndarray, ys: np.ndarray, zs: np.ndarray, **kw) -> object:
+        """:meth:`to_tensor` as a CuPy array (requires CuPy; zero-copy through DLPack)."""
+        out = kw.pop("out", None)
+        t = self.to_tensor(xs, ys, zs, out=None if out is None else _from_cupy(out), **kw)
+        return _to_cupy(t)
 
     def sample_into(self, volume: Volume, *, supersamp_factor: int = 1) -> Volume:
         """Add the phantom, point-sampled at ``volume``'s voxel centres (with
