@@ -9,8 +9,11 @@ ABI in include/aprict_b200.h.
 """
 
 from .volume import FBVolume, Volume  # noqa: I001  (iterators import Volume from here)
-from . import cb, iterators
+from . import cb, iterators, phantoms, volume
+from . import _structs as dtypes
+from . import gbc, geometry, recon
 
 __version__ = "0.1.0"
 
-__all__ = ["FBVolume", "Volume", "__version__", "cb", "iterators"]
+__all__ = ["FBVolume", "Volume", "__version__", "cb", "dtypes", "gbc", "geometry", "iterators", "phantoms", "recon",
+           "volume"]
