@@ -1,7 +1,7 @@
 """Launch-shape autotuner.
 
 Times a few candidate launch shapes of the forward projector (detector tile
-height, warp patch shape) and the backprojector (voxels per thread, size of the brick-ordered
+height, warp patch shape, neighbouring views per tile) and the backprojector (voxels per thread, size of the brick-ordered
 wave) on the caller's own problem with CUDA events, keeps the fastest, and
 applies it through ``aprict_b200_set_tuning``. Results never depend on these
 knobs; only speed does. Choices are cached per problem signature (in memory,
@@ -20,9 +20,10 @@ from . import _lib
 from .cb import flatpanel as fp
 from .volume import Volume
 
-KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V = 0, 1, 2, 3
+KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V, KEY_FP_VIEWS, KEY_FP_WARP_VIEWS = 0, 1, 2, 3, 4, 5
 FP_TILE_V = (8, 16, 32)
 FP_WARP_V = (8, 16, 32)
+FP_VIEWS = ((1, 1), (2, 1), (2, 2), (4, 1), (4, 2))  # (views per tile, views inside a warp)
 BP_XB = (2, 4, 8)
 BP_WAVE = (2, 3, 4, 6)
 
@@ -40,6 +41,8 @@ def current() -> dict:
     return {
         "fp_tile_v": lib.aprict_b200_get_tuning(KEY_FP_TILE_V),
         "fp_warp_v": lib.aprict_b200_get_tuning(KEY_FP_WARP_V),
+        "fp_views": lib.aprict_b200_get_tuning(KEY_FP_VIEWS),
+        "fp_warp_views": lib.aprict_b200_get_tuning(KEY_FP_WARP_VIEWS),
         "bp_xb": lib.aprict_b200_get_tuning(KEY_BP_XB),
         "bp_wave": lib.aprict_b200_get_tuning(KEY_BP_WAVE),
     }
@@ -49,6 +52,8 @@ def apply(choice: dict) -> None:
     """Apply a choice returned by :func:`tune`."""
     _set(KEY_FP_TILE_V, choice.get("fp_tile_v", 0))
     _set(KEY_FP_WARP_V, choice.get("fp_warp_v", 0))
+    _set(KEY_FP_VIEWS, choice.get("fp_views", 0))
+    _set(KEY_FP_WARP_VIEWS, choice.get("fp_warp_views", 0))
     _set(KEY_BP_XB, choice.get("bp_xb", 0))
     _set(KEY_BP_WAVE, choice.get("bp_wave", 0))
 
@@ -101,6 +106,8 @@ def tune(
     scratch_p = projs.zeroed_copy()
     cfg_fp = fp.ConfigProject()
     times = {}
+    _set(KEY_FP_VIEWS, 1)
+    _set(KEY_FP_WARP_VIEWS, 1)
     for tv in FP_TILE_V:
         for wv in FP_WARP_V:
             if wv > tv:
@@ -110,7 +117,16 @@ def tune(
             times[(tv, wv)] = _time(lambda: fp.project(cfg_fp, volume, scratch_p), reps)
     best_fp = min(times, key=times.get)
     choice["fp_tile_v"], choice["fp_warp_v"] = best_fp
-    choice["fp_ms"] = round(times[best_fp], 4)
+    _set(KEY_FP_TILE_V, best_fp[0])
+    _set(KEY_FP_WARP_V, best_fp[1])
+    vtimes = {(1, 1): times[best_fp]}
+    for tw, ww in FP_VIEWS[1:]:
+        _set(KEY_FP_VIEWS, tw)
+        _set(KEY_FP_WARP_VIEWS, ww)
+        vtimes[(tw, ww)] = _time(lambda: fp.project(cfg_fp, volume, scratch_p), reps)
+    best_v = min(vtimes, key=vtimes.get)
+    choice["fp_views"], choice["fp_warp_views"] = best_v
+    choice["fp_ms"] = round(vtimes[best_v], 4)
     if cfg_bp is not None:
         scratch_v = volume.zeroed_copy()
         best = None

@@ -7,10 +7,11 @@
 // per (view, pixel); ssu x ssv sub-rays averaged as in :381-407; result
 // scaled by multiply_before_adding (:394) and accumulated (:411).
 //
-// B200 layout: a CTA covers a 2-D detector tile of one view and each warp a
-// 4 (u) x 8 (v) pixel patch (2 x 16 or 1 x 32 as tuned), so the rays of a warp
-// are spatially coherent and their voxel gathers hit the same L1 lines; 8
-// consecutive v per row make the output access one 32-byte sector.
+// B200 layout: a CTA covers a 2-D detector tile of one view (or of 2 or 4
+// neighbouring views, as tuned) and each warp a 4 (u) x 8 (v) pixel patch
+// (2 x 16 or 1 x 32 as tuned), so the rays of a warp are spatially coherent
+// and their voxel gathers hit the same L1 lines; 8 consecutive v per row make
+// the output access one 32-byte sector.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,49 +25,73 @@ namespace ab_fp {
 constexpr int kThreads = 256;
 
 struct TileMap {
-    int tile_u, tile_v;  // tile extents in pixels
-    int warp_v;          // lanes of a warp along v (warp patch: 32/warp_v along u)
-    int ntu, ntv;        // number of tiles along u, v
+    int tile_w, tile_u, tile_v;  // tile extents: views, pixels along u, pixels along v
+    int warp_w, warp_u, warp_v;  // a warp's patch (product 32)
+    int ntw, ntu, ntv;           // number of tiles along views, u, v
+    uint64_t units() const { return (uint64_t)ntw * ntu * ntv; }
 };
 
 // Tile shapes: tv == 1 -> one detector row per tile (used when nv < 8);
-// otherwise warps are 4 (u) x 8 (v) patches.
-inline TileMap make_tiles(uint32_t nu, uint32_t nv) {
+// otherwise warps are 1 (view) x 4 (u) x 8 (v) patches of a 4 x 4 x 16
+// tile: four neighbouring views, one per pair of warps. Rays of neighbouring
+// views cross nearly the same voxels, so more of their gathers hit the same
+// L1 lines. The autotuner may change the tile height (8, 16, 32), the warp
+// patch height (16, 32), the views per tile (1, 2, 4) and put 2 or 4 views
+// inside each warp's patch.
+inline TileMap make_tiles(uint32_t nu, uint32_t nv, uint32_t n_views) {
     TileMap t;
     t.tile_v = nv >= 16 ? 16 : (nv >= 8 ? 8 : 1);
     const int want = ab_tuning_get(AB_TUNE_FP_TILE_V);  // autotuner override: 8, 16 or 32
     if ((want == 8 || want == 16 || want == 32) && nv >= 8) t.tile_v = want;
-    // Warp patch: 4 (u) x 8 (v) by default; the autotuner may try 2 x 16 or 1 x 32.
     const int wv = ab_tuning_get(AB_TUNE_FP_WARP_V);
     t.warp_v = (wv == 16 || wv == 32) ? wv : 8;
-    if (t.tile_v > 1 && t.warp_v > t.tile_v) t.tile_v = t.warp_v;
-    t.tile_u = kThreads / t.tile_v;
+    const int tw = ab_tuning_get(AB_TUNE_FP_VIEWS), ww = ab_tuning_get(AB_TUNE_FP_WARP_VIEWS);
+    t.tile_w = (tw == 1 || tw == 2) ? tw : 4;  // 4 by default: measured 2 % faster than 1 on a 256^3 volume
+    t.warp_w = (ww == 2 || ww == 4) ? ww : 1;
+    if (t.tile_v == 1) {
+        t.tile_w = t.warp_w = 1;
+        t.warp_v = 1;
+    } else {
+        if (t.warp_v > t.tile_v) t.tile_v = t.warp_v;
+        if (t.warp_w > t.tile_w) t.warp_w = t.tile_w;
+        while (t.warp_w * t.warp_v > 32) t.warp_w /= 2;
+        while (t.tile_w * t.tile_v > kThreads / (32 / (t.warp_w * t.warp_v))) t.tile_w /= 2;
+        if (t.warp_w > t.tile_w) t.warp_w = t.tile_w;
+    }
+    t.warp_u = 32 / (t.warp_w * t.warp_v);
+    t.tile_u = kThreads / (t.tile_w * t.tile_v);
     t.ntu = (int)((nu + t.tile_u - 1) / t.tile_u);
     t.ntv = (int)((nv + t.tile_v - 1) / t.tile_v);
+    t.ntw = (int)((n_views + t.tile_w - 1) / t.tile_w);
     return t;
 }
 
-// Blocks are ordered (detector row band, view, column tile) with the band
-// slowest: the CTAs resident at one time work on one band of rows of some
-// tens of views, whose rays cross only a slab of the volume, so the volume
-// data they gather stays in L2 (rather than whole views, which touch all of it).
-__device__ __forceinline__ void block_tile(const TileMap &tm, uint32_t n_views, uint32_t b, int &view, int &iu,
+// Blocks are ordered (detector row band, view group, column tile) with the
+// band slowest: the CTAs resident at one time work on one band of rows of
+// some tens of views, whose rays cross only a slab of the volume, so the
+// volume data they gather stays in L2 (rather than whole views, which touch
+// all of it). False when the thread has no ray (past the last view).
+__device__ __forceinline__ bool block_tile(const TileMap &tm, uint32_t n_views, uint32_t b, int &view, int &iu,
                                            int &iv) {
     const int tu = (int)(b % (uint32_t)tm.ntu);
     const uint32_t rest = b / (uint32_t)tm.ntu;
-    view = (int)(rest % n_views);
-    const int tv = (int)(rest / n_views);
+    const int tw = (int)(rest % (uint32_t)tm.ntw);
+    const int tv = (int)(rest / (uint32_t)tm.ntw);
     const int t = threadIdx.x;
     if (tm.tile_v == 1) {
+        view = tw;
         iu = tu * tm.tile_u + t;
         iv = tv;
     } else {
         const int lane = t & 31, warp = t >> 5;
-        const int wv_per = tm.tile_v / tm.warp_v;  // warps along v in the tile
-        const int wu = warp / wv_per, wv = warp % wv_per;
-        iu = tu * tm.tile_u + wu * (32 / tm.warp_v) + lane / tm.warp_v;
-        iv = tv * tm.tile_v + wv * tm.warp_v + lane % tm.warp_v;
+        const int lv = lane % tm.warp_v, lu = (lane / tm.warp_v) % tm.warp_u, lw = lane / (tm.warp_v * tm.warp_u);
+        const int nwv = tm.tile_v / tm.warp_v, nwu = tm.tile_u / tm.warp_u;
+        const int wv = warp % nwv, wu = (warp / nwv) % nwu, ww = warp / (nwv * nwu);
+        view = tw * tm.tile_w + ww * tm.warp_w + lw;
+        iu = tu * tm.tile_u + wu * tm.warp_u + lu;
+        iv = tv * tm.tile_v + wv * tm.warp_v + lv;
     }
+    return view < (int)n_views;
 }
 
 // L2 policy for the volume gathers: keep the volume resident (evict_last)
@@ -115,8 +140,7 @@ struct FPScan {
 template <typename Off, bool SS1>
 __device__ __forceinline__ void fp_tile(const FPScan<Off> &S, uint32_t b) {
     int view, iu, iv;
-    block_tile(S.tm, S.n_views, b, view, iu, iv);
-    if (iu >= (int)S.nu || iv >= (int)S.nv) return;
+    if (!block_tile(S.tm, S.n_views, b, view, iu, iv) || iu >= (int)S.nu || iv >= (int)S.nv) return;
     const uint64_t pol = l2_evict_last_policy();
     bool bad = false;
     float tot;
@@ -196,9 +220,9 @@ inline FPScan<Off> make_fpscan(const aprict_proj_spec *specs, const aprict_proj_
     S.mba = cfg->multiply_before_adding;
     S.ssu = (int)cfg->ssu;
     S.ssv = (int)cfg->ssv;
-    S.tm = make_tiles(pd->nu, pd->nv);
+    S.tm = make_tiles(pd->nu, pd->nv, pd->n_views);
     S.status = status;
-    units = (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) ? 0 : (uint64_t)S.tm.ntu * S.tm.ntv * pd->n_views;
+    units = (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) ? 0 : S.tm.units();
     return S;
 }
 

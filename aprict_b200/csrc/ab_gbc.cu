@@ -60,11 +60,16 @@ SoftWin soft_win(double a, double b) {
 
 // The window at s = sqrt(s2), s = sin|angle| in [0, 1]: compared on squares,
 // a square root only inside the soft band.
+// The soft band's cubic at s = sqrt(s2).
+__device__ __forceinline__ float soft_band(float s2, const SoftWin &w) {
+    const float x = w.gamma * sqrtf(s2) - w.chi;
+    return fmaxf(0.f, fminf(1.f, 3.f * x * x - 2.f * x * x * x));
+}
+
 __device__ __forceinline__ float soft_of_sin2(float s2, const SoftWin &w) {
     if (s2 > w.sa2) return 0.f;
     if (s2 < w.sab2) return 1.f;
-    const float x = w.gamma * sqrtf(s2) - w.chi;
-    return fmaxf(0.f, fminf(1.f, 3.f * x * x - 2.f * x * x * x));
+    return soft_band(s2, w);
 }
 
 // GBC weight (eq. 23 of the GBC method with the soft windows,
@@ -207,36 +212,71 @@ __global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPPa
 // (the first with weight 1/2) and num_ang source angles t in [0, pi) of the
 // weight of the voxel (r, 0, 0) for the source (cos t, sin t, z), times
 // 4 z_max pi / (num_z num_ang) (get_GBC_weight_integ, CB_backproject.cu:1108-1168).
-// kSPT (height, angle) samples per thread, held in registers across the
-// radii; per radius an FP64 block sum and one atomic add.
-constexpr int kSPT = 8;  // samples per thread of the weight integral
+//
+// The weight factorises: with the voxel at (r, 0, 0) and the source at
+// (cos t, sin t, z), ell and the horizontal angle depend on (r, t) only, so
+//   w(r, t, z) = A(r, t) cos^3(theta) s_v(sin^2 theta),
+//   A = c / max(1e-9, c^2 + (c - ell)^2) s_h(1 - c^2),
+//   cos theta = ell / h, sin^2 theta = z^2 / h^2, h^2 = ell^2 + z^2.
+// One thread per (radius, angle) evaluates A once and runs the height loop
+// (a reciprocal square root and a few multiplies per sample). sin^2 theta
+// grows with z, so the loop stops at the first height past the vertical
+// window, where the window is 0 (it reaches 0 continuously at its edge).
+// Heights are summed in FP32 in runs of 64, the runs in FP64; per radius an
+// FP64 block sum over angles and one atomic add.
+constexpr int kZRun = 64;  // heights per FP32 partial sum
+
+// sum over heights iz = 0 .. num_z - 1 (iz = 0 with weight 1/2) of
+// cos^3(theta) s_v(sin^2 theta), for horizontal distance ell.
+__device__ double height_sum(float ell, int num_z, float dz, const SoftWin &v) {
+    const float e2 = ell * ell, e3 = e2 * ell;
+    double tot = 0.5 * (double)soft_of_sin2(0.f, v);  // z = 0: cos theta = 1, sin theta = 0
+    if (e3 == 0.f) return tot;  // ell = 0: cos theta = 0 at every z > 0
+    bool done = false;
+    for (int base = 1; base < num_z && !done; base += kZRun) {
+        const int stop = min(num_z, base + kZRun);
+        float part = 0.f;
+        for (int iz = base; iz < stop; ++iz) {
+            const float z = (float)iz * dz;
+            const float z2 = z * z;
+            const float ih = rsqrtf(e2 + z2);
+            const float ih2 = ih * ih;
+            const float s2 = z2 * ih2;
+            if (s2 > v.sa2) {
+                done = true;
+                break;
+            }
+            const float win = s2 < v.sab2 ? 1.f : soft_band(s2, v);
+            part = fmaf(e3 * ih * ih2, win, part);
+        }
+        tot += (double)part;
+    }
+    return tot;
+}
 
 __global__ void __launch_bounds__(kGThreads) k_gbc_weight_integ(const float *r_on_R, int nr, double *out, int num_z,
                                                                 int num_ang, GbcSoft S, float tan_v) {
     __shared__ double warp_sums[kGThreads / 32];
-    const int64_t n = (int64_t)num_z * num_ang;
     const float maxz = tan_v * (1.f + r_on_R[nr - 1]);  // tan(soft_vartheta_v) (1 + r_max)
-    // this thread's samples: source position and end weight (0 past the end)
-    float sx[kSPT], sy[kSPT], sz[kSPT], half[kSPT];
-#pragma unroll
-    for (int k = 0; k < kSPT; ++k) {
-        const int64_t e = ((int64_t)blockIdx.x * kSPT + k) * kGThreads + threadIdx.x;
-        const bool live = e < n;
-        const int iz = live ? (int)(e / num_ang) : 0, ia = live ? (int)(e % num_ang) : 0;
-        sz[k] = maxz * (float)iz / (float)(num_z - 1);
-        const float t = (float)ia / (float)num_ang * 3.1415926535898f;
-        sx[k] = cosf(t);
-        sy[k] = sinf(t);
-        half[k] = !live ? 0.f : (iz == 0 ? 0.5f : 1.f);
-    }
+    const float dz = maxz / (float)(num_z - 1);
+    const int ia = blockIdx.x * kGThreads + threadIdx.x;
+    const bool live = ia < num_ang;
+    const float t = (float)(live ? ia : 0) / (float)num_ang * 3.1415926535898f;
+    const float ct = cosf(t), st = sinf(t);
     const double mult = (double)((4.f * maxz * 3.1415926535898f) / ((float)num_z * (float)num_ang));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int r = 0; r < nr; ++r) {
-        const float rr = r_on_R[r];
+    for (int r = blockIdx.y; r < nr; r += gridDim.y) {
         double w = 0.0;
-#pragma unroll
-        for (int k = 0; k < kSPT; ++k)
-            if (half[k] != 0.f) w += (double)(gbc_weight(1.f, rr, 0.f, 0.f, sx[k], sy[k], sz[k], 1.f, S) * half[k]);
+        if (live) {
+            const float rx = r_on_R[r] - ct, ry = -st;  // voxel minus source, in units of R
+            const float q = rx * rx + ry * ry;
+            const float rq = rsqrtf(q);
+            const float ell = q > 0.f ? q * rq : 0.f;
+            const float c = fmaxf(0.f, fminf(1.f, fabsf((rx * ct + ry * st) * rq)));  // NaN at q = 0 -> 1
+            const float d = c - ell;
+            const float a = __fdividef(c, fmaxf(1e-9f, c * c + d * d)) * soft_of_sin2(fmaxf(0.f, 1.f - c * c), S.h);
+            if (a != 0.f) w = (double)a * height_sum(ell, num_z, dz, S.v);
+        }
 #pragma unroll
         for (int k = 16; k > 0; k >>= 1) w += __shfl_xor_sync(0xffffffffu, w, k);
         if (lane == 0) warp_sums[warp] = w;
@@ -423,11 +463,9 @@ extern "C" int aprict_b200_gbc_weight_integral(const float *r_on_R_dev, int32_t 
     if (!finite_soft(cfg)) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "non-finite soft windows");
     const GbcSoft S{soft_win(cfg->soft_vartheta_v, cfg->soft_vartheta_v_softspan),
                     soft_win(cfg->soft_vartheta_h, cfg->soft_vartheta_h_softspan)};
-    const int64_t n = (int64_t)num_z * num_ang;
-    const int64_t per_block = (int64_t)kGThreads * kSPT;
-    k_gbc_weight_integ<<<(unsigned)((n + per_block - 1) / per_block), kGThreads, 0,
-                         reinterpret_cast<cudaStream_t>(stream)>>>(r_on_R_dev, n_r, out_dev, num_z, num_ang, S,
-                                                              (float)tan((double)cfg->soft_vartheta_v));
+    const dim3 grid((unsigned)((num_ang + kGThreads - 1) / kGThreads), (unsigned)min(n_r, 65535));
+    k_gbc_weight_integ<<<grid, kGThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        r_on_R_dev, n_r, out_dev, num_z, num_ang, S, (float)tan((double)cfg->soft_vartheta_v));
     return ab_cuda_check(cudaGetLastError(), "gbc_weight_integral launch");
 }
 

@@ -25,7 +25,9 @@ enum {
     AB_TUNE_BP_XB = 1,      // backprojector voxels per thread (0 = auto = 2, 2, 4)
     AB_TUNE_BP_WAVE = 2,    // backprojector super-brick size in CTAs per SM (0 = auto = 3)
     AB_TUNE_FP_WARP_V = 3,  // forward projector lanes of a warp along v (0 = auto = 8, 8, 16, 32)
-    AB_TUNE_COUNT = 4
+    AB_TUNE_FP_VIEWS = 4,   // forward projector views per tile (0 = auto = 4, 1, 2, 4)
+    AB_TUNE_FP_WARP_VIEWS = 5,  // forward projector views inside a warp's patch (0 = auto = 1, 1, 2, 4)
+    AB_TUNE_COUNT = 6
 };
 int ab_tuning_get(int key);
 

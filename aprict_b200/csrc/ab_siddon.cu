@@ -31,8 +31,7 @@ __global__ void __launch_bounds__(kThreads, 4)
                           ab_pstrides ps, const float *__restrict__ projs, ab_grid<Off> g, float *vol, float svf,
                           float mba, int ssu, int ssv, TileMap tm, uint32_t *status) {
     int view, iu, iv;
-    block_tile(tm, n_views, blockIdx.x, view, iu, iv);
-    if (iu >= (int)nu || iv >= (int)nv) return;
+    if (!block_tile(tm, n_views, blockIdx.x, view, iu, iv) || iu >= (int)nu || iv >= (int)nv) return;
     const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
     const float p = projs[o];
     if (p == 0.f) return;
@@ -87,10 +86,10 @@ extern "C" int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev
     int rc = fp_check(specs_dev, pd, projs_dev, vd, vol_dev, cfg);
     if (rc != APRICT_OK) return rc;
     if (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) return APRICT_OK;
-    const TileMap tm = make_tiles(pd->nu, pd->nv);
+    const TileMap tm = make_tiles(pd->nu, pd->nv, pd->n_views);
     const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const uint64_t nblocks = (uint64_t)tm.ntu * tm.ntv * pd->n_views;
+    const uint64_t nblocks = tm.units();
     if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
     if (small_volume(vd)) {
         k_backproject_scatter<int32_t><<<(unsigned)nblocks, kThreads, 0, st>>>(

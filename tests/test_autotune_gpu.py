@@ -1,7 +1,8 @@
 """Launch-shape knobs change speed only: every knob value gives the same result.
 
 The forward projector computes each ray independently of the tile it sits in,
-so its output is bit-identical across tile heights and warp patch shapes. The backprojector's wave
+so its output is bit-identical across tile heights, warp patch shapes and
+views per tile. The backprojector's wave
 size only reorders CTAs, so it is bit-identical too; its voxels-per-thread
 count changes where the per-view affine terms are stepped from (a thread's
 first voxel), so results across that knob agree to float rounding (rel L2
@@ -41,12 +42,30 @@ def test_projector_tile_shapes_are_bit_identical(restore_knobs) -> None:
     outs = []
     for tv in autotune.FP_TILE_V:
         for wv in autotune.FP_WARP_V:
-            autotune.apply({"fp_tile_v": tv, "fp_warp_v": wv})
-            ps = fp.ProjectionSet(pg, data=None)
-            fp.project(fp.ConfigProject(ssu=2), vol, ps, block=True)
-            outs.append(ps.data.cpu().numpy())
+            for tw, ww in autotune.FP_VIEWS:
+                autotune.apply({"fp_tile_v": tv, "fp_warp_v": wv, "fp_views": tw, "fp_warp_views": ww})
+                ps = fp.ProjectionSet(pg, data=None)
+                fp.project(fp.ConfigProject(ssu=2), vol, ps, block=True)
+                outs.append(ps.data.cpu().numpy())
     for o in outs[1:]:
         assert np.array_equal(o, outs[0])
+    # an odd view count leaves the last multi-view tile part empty; the
+    # ray-driven adjoint shares the tiles (atomic sums: equal to rounding)
+    pg5 = circular(5, 120, 120, 0.537, 52, 56)
+    y = fp.ProjectionSet(pg5, data=np.random.default_rng(3).random((5, 52, 56), dtype=np.float32))
+    outs, adj = [], []
+    for tw, ww in autotune.FP_VIEWS:
+        autotune.apply({"fp_views": tw, "fp_warp_views": ww})
+        ps = fp.ProjectionSet(pg5, data=None)
+        fp.project(fp.ConfigProject(), vol, ps, block=True)
+        outs.append(ps.data.cpu().numpy())
+        v = Volume.zeros(SHAPE, voxwid=1.0)
+        fp.backproject_adjoint(fp.ConfigProject(), v, y, block=True)
+        adj.append(v.as_numpy())
+    for o, a in zip(outs[1:], adj[1:]):
+        assert np.array_equal(o, outs[0])
+        assert rel_l2(a, adj[0]) <= 1e-6
+    assert np.linalg.norm(adj[0]) > 0
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(fast_approx=True, approx_mode_bilinear_interpolate=True), dict(fast_approx=True)])
@@ -79,6 +98,7 @@ def test_tune_picks_allowed_values_and_caches(restore_knobs, tmp_path) -> None:
     cache = tmp_path / "tune.json"
     choice = autotune.tune(ps, vol, cfg_bp=fp.ConfigBackproject(), cache_file=cache)
     assert choice["fp_tile_v"] in autotune.FP_TILE_V and choice["fp_warp_v"] in autotune.FP_WARP_V
+    assert (choice["fp_views"], choice["fp_warp_views"]) in autotune.FP_VIEWS
     assert choice["bp_xb"] in autotune.BP_XB and choice["bp_wave"] in autotune.BP_WAVE
     assert autotune.current()["fp_tile_v"] == choice["fp_tile_v"]
     assert torch.equal(ps.data, before_p) and torch.equal(vol.data, before_v)
