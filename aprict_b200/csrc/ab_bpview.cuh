@@ -39,6 +39,11 @@ struct ab_bpview {
     // ab_fp32_pixel_error_bound); above it the choice is made in FP64.
     float tie_u, tie_v;
     float sxw, syw;  // source position (world x, y), for the cone-cylinder weighting presets
+    // Certainly off the detector: |fu - cu0| > out_ru (or v) puts the nearest
+    // pixel out of range in FP32 and in exact arithmetic alike (the half-width
+    // plus the FP32 error bound); out_ru + 1/2 does the same for all four
+    // bilinear taps.
+    float out_ru, out_rv;
 };
 
 // A priori bound on the error of the FP32 detector coordinate f = N(x)/D(x)
@@ -127,6 +132,8 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
     const double ev = 1.5 * ab_fp32_pixel_error_bound(Av, ab_dot(Av, c0s), n, bdn, half_ext, fmax);
     o.tie_u = (float)(0.5 - (eu > 1e-4 ? eu : 1e-4));
     o.tie_v = (float)(0.5 - (ev > 1e-4 ? ev : 1e-4));
+    o.out_ru = (float)(0.5 * (double)sp.nu + (eu > 1e-4 ? eu : 1e-4) + 1e-3);
+    o.out_rv = (float)(0.5 * (double)sp.nv + (ev > 1e-4 ? ev : 1e-4) + 1e-3);
     o.sxw = (float)s.x;
     o.syw = (float)s.y;
     return true;
