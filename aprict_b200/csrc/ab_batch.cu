@@ -140,13 +140,17 @@ __global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __gr
 // default, two for slice stacks (as the single-scan launch).
 constexpr int batch_xb(int ord, bool exact) { return ord == 2 ? 2 : ab_bp::default_xb(exact); }
 
+// The batch kernel skips, in every fast mode, the views whose projection of
+// a brick misses the detector: batches mix helical and circular scans, and
+// the helical ones leave most of a volume off each view's detector (48
+// uneven scans: 326.6 -> 265.3 ms per batched backprojection).
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
 __global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb(ORD, EXACT), EXACT))
     k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
     __shared__ ab_bp::BPSmem<EXACT, BILIN, batch_xb(ORD, EXACT)> sm;
     uint32_t unit;
     int s;
-    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD, EXACT)>(A.scans[s], unit, sm);
+    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD, EXACT), true>(A.scans[s], unit, sm);
     retire(A.g);
 }
 

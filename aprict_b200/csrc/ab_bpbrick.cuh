@@ -253,7 +253,7 @@ struct BPSmem {
 // One backprojection work unit: brick `brick` (brick order) of the volume,
 // all views. Every thread of the CTA calls it with the same brick; it contains
 // __syncthreads and returns uniformly.
-template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
+template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB, bool SKIP = RAYCAST>
 __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSmem<EXACT, BILIN, XB> &sm) {
     static_assert(XB == 2 || XB == 4 || XB == 8, "XB is 2, 4 or 8");
     constexpr int kXB = XB, kKB = q_kbits<XB>();
@@ -311,12 +311,13 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
         any_live |= ok;
     }
 
-    // Direct-raycast mode (the cone-cylinder FBP's, whose views each see only
-    // a slab of the volume) skips the views whose projection of the brick
-    // misses the detector, and leaves voxel-views certainly off the detector
-    // out of the second pass. The other modes keep the plain loop: measured
-    // 3 % slower with the skip on a circular scan that never misses.
-    constexpr bool kSkip = RAYCAST;
+    // SKIP (by default in the direct-raycast mode, the cone-cylinder FBP's,
+    // whose views each see only a slab of the volume): skip the views whose
+    // projection of the brick misses the detector, and leave voxel-views
+    // certainly off the detector out of the second pass. The one-scan kernel's
+    // other modes keep the plain loop: measured 3 % slower with the skip on a
+    // circular scan that never misses.
+    constexpr bool kSkip = SKIP && !EXACT;
     // The brick's box relative to the volume centre (voxel faces, clipped to
     // the volume): every sub-sample of its voxels lies inside. Kept in shared
     // memory for the per-view off-detector test (ordered by the chunk loop's

@@ -106,8 +106,13 @@ struct GbcParams {
     float pos000[3];  // world centre of voxel (0, 0, 0): corner + voxwid / 2
 };
 
+// Resident CTAs per SM: the kernel is bound by the latency of its detector
+// gathers, and at the unconstrained ~105 registers only 2 CTAs fit; a few
+// registers spilled (view derivation, FP64 tie refinement) cost less than the
+// lost occupancy (198^3 x 360 views: bilinear 22.7 -> 17.2 ms at 3 CTAs,
+// nearest 19.7 -> 12.9 ms at 4).
 template <bool BILIN>
-__global__ void __launch_bounds__(kGThreads) k_backproject_gbc(const ab_bp::BPParams P, const GbcParams G,
+__global__ void __launch_bounds__(kGThreads, BILIN ? 3 : 4) k_backproject_gbc(const ab_bp::BPParams P, const GbcParams G,
                                                                int order_f) {
     using namespace ab_bp;
     __shared__ ab_bpview sv[kGChunk];
