@@ -58,18 +58,25 @@ SoftWin soft_win(double a, double b) {
     return w;
 }
 
-// The window at s = sqrt(s2), s = sin|angle| in [0, 1]: compared on squares,
-// a square root only inside the soft band.
-// The soft band's cubic at s = sqrt(s2).
-__device__ __forceinline__ float soft_band(float s2, const SoftWin &w) {
-    const float x = w.gamma * sqrtf(s2) - w.chi;
+// The soft band's cubic at s = sin|angle|.
+__device__ __forceinline__ float soft_cubic(float s, const SoftWin &w) {
+    const float x = w.gamma * s - w.chi;
     return fmaxf(0.f, fminf(1.f, 3.f * x * x - 2.f * x * x * x));
 }
 
+// The window at s = sqrt(s2), s = sin|angle| in [0, 1]: compared on squares,
+// a square root only inside the soft band.
 __device__ __forceinline__ float soft_of_sin2(float s2, const SoftWin &w) {
     if (s2 > w.sa2) return 0.f;
     if (s2 < w.sab2) return 1.f;
-    return soft_band(s2, w);
+    return soft_cubic(sqrtf(s2), w);
+}
+
+// The same window when s itself is at hand (s2 = s * s): no square root.
+__device__ __forceinline__ float soft_of_sin(float s, float s2, const SoftWin &w) {
+    if (s2 > w.sa2) return 0.f;
+    if (s2 < w.sab2) return 1.f;
+    return soft_cubic(s, w);
 }
 
 // GBC weight (eq. 23 of the GBC method with the soft windows,
@@ -94,9 +101,9 @@ __device__ float gbc_weight(float inv_R, float px, float py, float pz, float sx,
     const float h2 = ell * ell + zr * zr;
     const float ih = rsqrtf(h2);
     const float cos_el = h2 > 0.f ? ell * ih : 1.f;
-    const float sin2_el = h2 > 0.f ? zr * zr * (ih * ih) : 0.f;
+    const float sin_el = h2 > 0.f ? fabsf(zr) * ih : 0.f;
     const float weight = __fdividef(cos_el * cos_el * cos_el * c, fmaxf(1e-9f, c * c + d * d));
-    return weight * soft_of_sin2(sin2_el, S.v) * soft_of_sin2(fmaxf(0.f, 1.f - c * c), S.h);
+    return weight * soft_of_sin(sin_el, sin_el * sin_el, S.v) * soft_of_sin2(fmaxf(0.f, 1.f - c * c), S.h);
 }
 
 struct GbcParams {
@@ -245,14 +252,14 @@ __device__ double height_sum(float ell, int num_z, float dz, const SoftWin &v) {
             const float z = (float)iz * dz;
             const float z2 = z * z;
             const float ih = rsqrtf(e2 + z2);
-            const float ih2 = ih * ih;
-            const float s2 = z2 * ih2;
+            const float s = z * ih;  // sin theta
+            const float s2 = s * s;
             if (s2 > v.sa2) {
                 done = true;
                 break;
             }
-            const float win = s2 < v.sab2 ? 1.f : soft_band(s2, v);
-            part = fmaf(e3 * ih * ih2, win, part);
+            const float win = s2 < v.sab2 ? 1.f : soft_cubic(s, v);
+            part = fmaf(e3 * ih * (ih * ih), win, part);
         }
         tot += (double)part;
     }
