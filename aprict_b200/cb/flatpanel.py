@@ -378,6 +378,18 @@ class ProjectionSet:
         self._specs_dev: torch.Tensor | None = None
         self._out_of_mem_counter: torch.Tensor | None = None
 
+    def _with_data(self, data: torch.Tensor) -> ProjectionSet:
+        """A ProjectionSet of this geometry over ``data`` (a device tensor of the same
+        shape), sharing the packed views and their device copy (no re-packing or upload)."""
+        _assert_flatpanel_geometry_consistency(self._proj_specs, data)
+        out = ProjectionSet.__new__(ProjectionSet)
+        out._proj_geom = self._proj_geom
+        out._proj_specs = self._proj_specs
+        out._data = data
+        out._specs_dev = self.specs_device()
+        out._out_of_mem_counter = None
+        return out
+
     @property
     def proj_geom(self) -> ProjGeom:
         """The geometry."""

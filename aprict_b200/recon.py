@@ -126,7 +126,12 @@ def fbp_fan_circ_batch(
     if not projs or len(projs) != len(volumes):
         msg = "one volume per sinogram, at least one"
         raise ValueError(msg)
-    geo = [fan_geometry(p.proj_geom) for p in projs]
+    # slices of one stack usually share one ProjGeom object: check each distinct one once
+    by_id: dict[int, tuple] = {}
+    for p in projs:
+        if id(p.proj_geom) not in by_id:
+            by_id[id(p.proj_geom)] = fan_geometry(p.proj_geom)
+    geo = [by_id[id(p.proj_geom)] for p in projs]
     m = projs[0].proj_geom.num_projs
     if any(not np.allclose(g, geo[0]) for g in geo) or any(p.proj_geom.num_projs != m for p in projs):
         msg = "batched fan FBP needs one fan geometry and view count for every slice"
@@ -141,7 +146,7 @@ def fbp_fan_circ_batch(
         fast_approx=True, cyl_mask_rad=support, Z_on_val_factor_power=-2, Z_on_val_factor_val=R,
         approx_mode_direct_raycast=True, approx_mode_bilinear_interpolate=interpolate,
     )
-    views = [fp.ProjectionSet(p.proj_geom, data=filtered[i * m : (i + 1) * m]) for i, p in enumerate(projs)]
+    views = [p._with_data(filtered[i * m : (i + 1) * m]) for i, p in enumerate(projs)]  # noqa: SLF001
     ScanBatch(volumes, views).backproject(cfg)
     return volumes
 
