@@ -35,7 +35,7 @@ static_assert(sizeof(aprict_forbild_shape) == 156, "FORBILD_Shape is 156 bytes i
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kChunk = 96;  // shapes per shared-memory chunk
+constexpr int kChunk = 128;  // shapes per shared-memory chunk (one chunk, one barrier round, up to 128 shapes)
 constexpr int kMaxU = 16;   // disjoint covered intervals tracked per ray
 
 struct QView {
@@ -481,8 +481,14 @@ TileMap make_tiles(uint32_t nu, uint32_t nv) {
     return t;
 }
 
+// 5 resident CTAs per SM (48 registers, the FP64 root solving spills some to
+// L1-resident local memory): the kernel waits on FP64 latencies, and the
+// unconstrained 106 registers fit only 2 CTAs. Measured on the 100-shape,
+// 720-view workload: 142.9 ms at 2 CTAs, 127.3 at 3, 113.4 at 4, 109.3 at 5,
+// 119.8 at 6 (96-shape chunks); 102.7 ms at 5 with 128-shape chunks, which
+// hold the 100 shapes in one chunk (warps wait at one barrier round, not two).
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_project_forbild(const aprict_proj_spec *__restrict__ specs,
+__global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_proj_spec *__restrict__ specs,
                                                                uint32_t n_views, uint32_t nu, uint32_t nv,
                                                                ab_pstrides ps, float *out,
                                                                const aprict_quadric *__restrict__ shapes,
