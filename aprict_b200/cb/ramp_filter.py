@@ -318,6 +318,28 @@ class FBPFilterer:
             return self.uniform_rng(-self._max_abs_rotation_angle, self._max_abs_rotation_angle, n)
         return force_rotation_angle * np.ones((n,), dtype=np.float32)
 
+    def _letterbox_matrix(self, angles: np.ndarray) -> np.ndarray:
+        """``_letterbox_columns`` of every angle at once, (len(angles), nv_e): the same
+        arithmetic elementwise, without a Python loop over the views."""
+        ang = np.asarray(angles)
+        if np.any(np.abs(ang) > self._max_abs_rotation_angle):
+            msg = "Invalid rotation angle entered."
+            raise ValueError(msg)
+        nv_e = self._expanded_2d_shape[1]
+        mid_index = (nv_e - 1) / 2
+        disc = self.L / self.physpixwid * np.sqrt(
+            np.maximum(np.square(np.cos(ang) / np.cos(self._max_abs_rotation_angle)) - 1, 0)
+        )
+        start, stop = mid_index - disc, mid_index + disc
+        i1, i2 = np.round(start).astype(np.int64), np.round(stop).astype(np.int64)
+        cols = np.arange(nv_e)[None, :]
+        w = ((cols >= i1[:, None]) & (cols <= i2[:, None])).astype(np.float64)
+        rows = np.arange(len(ang))
+        same = i1 == i2
+        w[rows, i1] = np.where(same, stop - start, (i1 + 1 / 2) - start)
+        w[rows[~same], i2[~same]] = (stop - (i2 - 1 / 2))[~same]
+        return w
+
     @staticmethod
     def _cs(angles_deg: np.ndarray) -> np.ndarray:
         # the library's chain: numpy.deg2rad in the angles' dtype, then math.cos / math.sin
@@ -341,7 +363,7 @@ class FBPFilterer:
             cs_bwd = torch.from_numpy(self._cs(180 / np.pi * ang)).cuda()
             colw = None
             if not hacky:
-                colw = torch.from_numpy(np.stack([self._letterbox_columns(x) for x in ang])).cuda()
+                colw = torch.from_numpy(self._letterbox_matrix(ang)).cuda()
             frame = torch.empty((b - a, nu_e, nv_e), dtype=torch.float32, device=data.device)
             src = data[a:b]
             d_src, d_frame = _desc(src), _desc(frame)  # kept alive across the calls

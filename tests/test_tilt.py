@@ -77,6 +77,11 @@ def test_frame_letterbox_and_draws(nu: int, nv: int, pw: float, L: float) -> Non
     nv_e = f._expanded_2d_shape[1]
     for ang in np.linspace(-zeta, zeta, 9).astype(np.float32)[1:-1]:
         np.testing.assert_array_equal(f._letterbox_columns(ang), T.letterbox_columns(ang, zeta, L, pw, nv_e))
+    # all views at once (the filter's path): the per-view values, bit for bit
+    many = _bare(nu, nv, pw, L, seed=5).uniform_rng(-zeta, zeta, 2000)
+    np.testing.assert_array_equal(f._letterbox_matrix(many), np.stack([f._letterbox_columns(a) for a in many]))
+    with pytest.raises(ValueError):
+        f._letterbox_matrix(np.array([0.0, 1.01 * zeta + 1e-3]))
     with pytest.raises(ValueError):
         f.get_letterbox_slice(1.01 * zeta + 1e-3)
     draws = f.uniform_rng(-zeta, zeta, 25)
