@@ -405,7 +405,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                               dot4(bq.nu, X, Y, Z)) * rD;
                         const float fv = fmaf(kf, (a2 == 0 ? bq.nv.x : (a2 == 1 ? bq.nv.y : bq.nv.z)) * vw,
                                               dot4(bq.nv, X, Y, Z)) * rD;
-                        float w = RAYCAST ? 1.f : bq.kfast * rD * rD;
+                        float w = RAYCAST ? 1.f : rD * rD;
                         if (needZ) {
                             const float Zk = fmaf(kf, (a2 == 0 ? bq.zl.x : (a2 == 1 ? bq.zl.y : bq.zl.z)) * vw,
                                                   dot4(bq.zl, X, Y, Z));
@@ -605,7 +605,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                 const float rD = rcp_fast(D);
                                 const float fu = fmaf(kf, dNu, Nu0) * rD;
                                 const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                float w = RAYCAST ? 1.f : b.kfast * rD * rD;
+                                float w = RAYCAST ? 1.f : rD * rD;
                                 if (needZ) {
                                     const float Zk = fmaf(kf, dZ, Zb);
                                     w *= zpow(P, b, Zk);

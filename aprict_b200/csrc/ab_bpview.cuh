@@ -25,7 +25,7 @@ struct ab_bpview {
     float4 nv;   // A_v.xyz, B_v
     float4 den;  // n.xyz,  (c0 - s).n
     float4 zl;   // Lhat.xyz, (c0 - s).Lhat  ->  Z(x) = distance along L = P - s
-    float kfast; // voxwid^3 Dn^2 / (|u||v|): fast-mode weight is kfast / den^2
+    float kfast; // voxwid^3 Dn^2 / (|u||v|), already folded into nu, nv, den (fast-mode weight 1 / den^2)
     float invL;  // 1 / |L|
     float halfu; // nu / 2
     float halfv; // nv / 2
@@ -108,9 +108,13 @@ AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, 
         *od = ab_bpview_d{{Au.x, Au.y, Au.z, ab_dot(Au, c0s)}, {Av.x, Av.y, Av.z, ab_dot(Av, c0s)},
                           {n.x, n.y, n.z, ab_dot(n, c0s)}};
     }
-    o.nu = make_float4((float)Au.x, (float)Au.y, (float)Au.z, (float)ab_dot(Au, c0s));
-    o.nv = make_float4((float)Av.x, (float)Av.y, (float)Av.z, (float)ab_dot(Av, c0s));
-    o.den = make_float4((float)n.x, (float)n.y, (float)n.z, (float)ab_dot(n, c0s));
+    // The three forms are scaled by 1 / sqrt(kfast): every ratio (the detector
+    // coordinates) is unchanged and the fast-mode weight kfast / D^2 becomes 1 / D'^2.
+    const double vw3 = (double)voxwid * (double)voxwid * (double)voxwid;
+    const double sc = 1.0 / sqrt(vw3 * Dn * Dn / (sqrt(uu) * sqrt(vv)));
+    o.nu = make_float4((float)(Au.x * sc), (float)(Au.y * sc), (float)(Au.z * sc), (float)(ab_dot(Au, c0s) * sc));
+    o.nv = make_float4((float)(Av.x * sc), (float)(Av.y * sc), (float)(Av.z * sc), (float)(ab_dot(Av, c0s) * sc));
+    o.den = make_float4((float)(n.x * sc), (float)(n.y * sc), (float)(n.z * sc), (float)(ab_dot(n, c0s) * sc));
     o.zl = make_float4((float)Lh.x, (float)Lh.y, (float)Lh.z, (float)ab_dot(Lh, c0s));
     const double vw = (double)voxwid;
     o.kfast = (float)(vw * vw * vw * Dn * Dn / (sqrt(uu) * sqrt(vv)));
