@@ -197,6 +197,24 @@ def run_ours(args) -> dict:
     torch.cuda.set_device(local)
     replicas.init("nccl")
     w = WORKLOADS[args.workload]
+    if args.workload == "fbpcyl":  # one direct-raycast backprojection of the cone-cylinder FBP per step
+        from aprict_b200 import geometry
+
+        n, m = w["n"], w["views"]
+        pg = geometry.cylinder_scan(n_views=m, R=w["R"], L_minus_R=w["LmR"], pix_at_iso=w["pix_at_iso"],
+                                    nu=w["det"], nv=w["det"], height=w["height"])
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(w["seed"])
+        ps = fp.ProjectionSet(pg, data=torch.rand((m, w["det"], w["det"]), device="cuda", generator=gen))
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pixwid = float(np.linalg.norm(pg.det_uvec[0]))
+        cfg = fp.ConfigBackproject(fast_approx=True, cyl_mask_rad=w["R"] * np.sin(np.arctan(pixwid * w["det"] / 2 / L)),
+                                   Z_on_val_factor_power=-3, Z_on_val_factor_val=w["R"], approx_mode_direct_raycast=True)
+        out = Volume.zeros((n, n, n), voxwid=w["voxwid"])
+        for _ in range(args.steps):
+            fp.backproject(cfg, out, ps)
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": args.steps}
     n = w["n"]
     pg, x_true = make_problem(w)
     b = simulate_data(pg, x_true, w)
@@ -848,6 +866,7 @@ def profile_kernels(args) -> dict:
 
     Launch order: 1 projection (simulated data), then ``--steps`` x (fused
     residual projection, all-view backprojection); nothing else runs on the GPU.
+    quadric, fbp64 and fbpcyl launch their own workload's kernels instead.
     """
     import torch
 
@@ -880,6 +899,24 @@ def profile_kernels(args) -> dict:
             fbp_fan_circ_batch(projs, vols, apodization="hann")
         torch.cuda.synchronize()
         return {"mode": "kernels", "workload": args.workload, "launches": 2 * args.steps}
+    if args.workload == "fbpcyl":  # one direct-raycast backprojection of the cone-cylinder FBP per step
+        from aprict_b200 import geometry
+
+        n, m = w["n"], w["views"]
+        pg = geometry.cylinder_scan(n_views=m, R=w["R"], L_minus_R=w["LmR"], pix_at_iso=w["pix_at_iso"],
+                                    nu=w["det"], nv=w["det"], height=w["height"])
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(w["seed"])
+        ps = fp.ProjectionSet(pg, data=torch.rand((m, w["det"], w["det"]), device="cuda", generator=gen))
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pixwid = float(np.linalg.norm(pg.det_uvec[0]))
+        cfg = fp.ConfigBackproject(fast_approx=True, cyl_mask_rad=w["R"] * np.sin(np.arctan(pixwid * w["det"] / 2 / L)),
+                                   Z_on_val_factor_power=-3, Z_on_val_factor_val=w["R"], approx_mode_direct_raycast=True)
+        out = Volume.zeros((n, n, n), voxwid=w["voxwid"])
+        for _ in range(args.steps):
+            fp.backproject(cfg, out, ps)
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": args.steps}
     n = w["n"]
     pg, x_true = make_problem(w)
     b = simulate_data(pg, x_true, w)
