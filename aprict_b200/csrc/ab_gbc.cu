@@ -252,7 +252,7 @@ __device__ double height_sum(float ell, int num_z, float dz, const SoftWin &v) {
             const float z = (float)iz * dz;
             const float z2 = z * z;
             const float ih = rsqrtf(e2 + z2);
-            const float s = z * ih;  // sin theta
+            const float s = fabsf(z) * ih;  // sin|theta| (z < 0 when the vertical window passes pi/2)
             const float s2 = s * s;
             if (s2 > v.sa2) {
                 done = true;

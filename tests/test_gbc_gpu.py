@@ -86,6 +86,24 @@ def test_weight_integral_matches_oracle() -> None:
     np.testing.assert_allclose(got, want, rtol=1e-5)
 
 
+@pytest.mark.parametrize(("r", "nz", "na", "soft"), [
+    (np.array([0.3]), 2, 1, SOFT),                      # smallest sampling
+    (np.array([0.0, 0.5, 0.9]), 3, 7, SOFT),
+    (np.linspace(0.0, 0.3, 5), 400, 300, (2.0, 0.1, 1.7, 0.3)),  # windows past pi/2: nothing cut
+    (np.linspace(0.0, 0.3, 4), 300, 257, (0.1, 0.2, 0.45, 0.05)),  # soft span wider than the window
+    (np.linspace(0.0, 0.3, 3), 300, 200, (1.7, 0.3, 0.45, 0.05)),  # past pi/2: heights below 0, soft band in use
+])
+def test_weight_integral_edges(r: np.ndarray, nz: int, na: int, soft: tuple) -> None:
+    cfg = fp.ConfigBackproject(fast_approx=True, backproj_weighting_preset=7, Z_on_val_factor_val=60.0,
+                               approx_mode_direct_raycast=True, soft_vartheta_v=soft[0],
+                               soft_vartheta_v_softspan=soft[1], soft_vartheta_h=soft[2],
+                               soft_vartheta_h_softspan=soft[3])
+    got = gbc.backproj_gbc_weight_integ_GPU(r, cfg, nz, na)
+    want = G.weight_integral(r.astype(np.float32), soft, nz, na)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6 * max(1.0, float(np.abs(want).max())))
+
+
 @pytest.mark.parametrize(("cone", "soft"), [(0.5, 0.05), (0.0, 0.0), (np.pi, 0.0), (1.2, 0.2)])
 def test_conebeam_filter_matches_oracle(cone: float, soft: float) -> None:
     rng = np.random.default_rng(int(cone * 10))
