@@ -197,6 +197,34 @@ def run_ours(args) -> dict:
     torch.cuda.set_device(local)
     replicas.init("nccl")
     w = WORKLOADS[args.workload]
+    if args.workload == "gbc":  # per step: one GBC backprojection of the padded volume, one weight integral
+        from aprict_b200 import geometry
+        from aprict_b200.gbc import weightinteg
+
+        n, m, vw = w["n"], w["views"], w["voxwid"]
+        pg = geometry.cylinder_scan(n_views=m, R=w["R"], L_minus_R=w["LmR"], pix_at_iso=w["pix_at_iso"],
+                                    nu=w["det"], nv=w["det"], height=w["height"])
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(w["seed"])
+        ps = fp.ProjectionSet(pg, data=torch.rand((m, w["det"], w["det"]), device="cuda", generator=gen))
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pixwid = float(np.linalg.norm(pg.det_uvec[0]))
+        nu = nv = w["det"]
+        cfg = fp.ConfigBackproject(
+            fast_approx=True, Z_on_val_factor_val=w["R"], backproj_weighting_preset=7, approx_mode_direct_raycast=True,
+            approx_mode_bilinear_interpolate=True,
+            soft_vartheta_v=float(np.arctan2(nv * pixwid / 2 - pixwid / 2, np.sqrt(L**2 + (nu * pixwid / 2 - pixwid / 2) ** 2))),
+            soft_vartheta_v_softspan=0.05, soft_vartheta_h=float(np.arctan2(nu * pixwid / 2 - pixwid / 2, L)),
+            soft_vartheta_h_softspan=0.05)
+        pad = 9 * (4 + int(np.ceil(n * 1.2 / 9)))
+        pad = pad if (pad - n) % 2 == 0 else pad + 9
+        vol, ws = Volume.zeros((pad,) * 3, voxwid=vw), Volume.zeros((pad,) * 3, voxwid=vw)
+        xs = vol.xs_ys_zs[0]
+        for _ in range(args.steps):
+            fp.backproject(cfg, vol, ps, secondary_volume=ws)
+            weightinteg.backproj_gbc_weight_integ_xygrid_GPU(xs, xs, w["R"], cfg)
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": 2 * args.steps}
     if args.workload == "fbpcyl":  # one direct-raycast backprojection of the cone-cylinder FBP per step
         from aprict_b200 import geometry
 
@@ -866,7 +894,7 @@ def profile_kernels(args) -> dict:
 
     Launch order: 1 projection (simulated data), then ``--steps`` x (fused
     residual projection, all-view backprojection); nothing else runs on the GPU.
-    quadric, fbp64 and fbpcyl launch their own workload's kernels instead.
+    quadric, fbp64, fbpcyl and gbc launch their own workload's kernels instead.
     """
     import torch
 
@@ -897,6 +925,34 @@ def profile_kernels(args) -> dict:
         vols = [Volume.zeros((w["n"], w["n"], 1), voxwid=w["voxwid"]) for _ in range(8)]
         for _ in range(args.steps):
             fbp_fan_circ_batch(projs, vols, apodization="hann")
+        torch.cuda.synchronize()
+        return {"mode": "kernels", "workload": args.workload, "launches": 2 * args.steps}
+    if args.workload == "gbc":  # per step: one GBC backprojection of the padded volume, one weight integral
+        from aprict_b200 import geometry
+        from aprict_b200.gbc import weightinteg
+
+        n, m, vw = w["n"], w["views"], w["voxwid"]
+        pg = geometry.cylinder_scan(n_views=m, R=w["R"], L_minus_R=w["LmR"], pix_at_iso=w["pix_at_iso"],
+                                    nu=w["det"], nv=w["det"], height=w["height"])
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(w["seed"])
+        ps = fp.ProjectionSet(pg, data=torch.rand((m, w["det"], w["det"]), device="cuda", generator=gen))
+        L = w["R"] + w["LmR"]  # noqa: N806
+        pixwid = float(np.linalg.norm(pg.det_uvec[0]))
+        nu = nv = w["det"]
+        cfg = fp.ConfigBackproject(
+            fast_approx=True, Z_on_val_factor_val=w["R"], backproj_weighting_preset=7, approx_mode_direct_raycast=True,
+            approx_mode_bilinear_interpolate=True,
+            soft_vartheta_v=float(np.arctan2(nv * pixwid / 2 - pixwid / 2, np.sqrt(L**2 + (nu * pixwid / 2 - pixwid / 2) ** 2))),
+            soft_vartheta_v_softspan=0.05, soft_vartheta_h=float(np.arctan2(nu * pixwid / 2 - pixwid / 2, L)),
+            soft_vartheta_h_softspan=0.05)
+        pad = 9 * (4 + int(np.ceil(n * 1.2 / 9)))
+        pad = pad if (pad - n) % 2 == 0 else pad + 9
+        vol, ws = Volume.zeros((pad,) * 3, voxwid=vw), Volume.zeros((pad,) * 3, voxwid=vw)
+        xs = vol.xs_ys_zs[0]
+        for _ in range(args.steps):
+            fp.backproject(cfg, vol, ps, secondary_volume=ws)
+            weightinteg.backproj_gbc_weight_integ_xygrid_GPU(xs, xs, w["R"], cfg)
         torch.cuda.synchronize()
         return {"mode": "kernels", "workload": args.workload, "launches": 2 * args.steps}
     if args.workload == "fbpcyl":  # one direct-raycast backprojection of the cone-cylinder FBP per step
