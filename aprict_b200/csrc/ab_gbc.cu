@@ -239,20 +239,40 @@ __global__ void __launch_bounds__(kGThreads, BILIN ? 3 : 4) k_backproject_gbc(co
 constexpr int kZRun = 64;  // heights per FP32 partial sum
 
 // sum over heights iz = 0 .. num_z - 1 (iz = 0 with weight 1/2) of
-// cos^3(theta) s_v(sin^2 theta), for horizontal distance ell.
+// cos^3(theta) s_v(sin^2 theta), for horizontal distance ell. sin^2 theta
+// grows with z, so the heights fall into three ranges: the window's flat part
+// (s_v = 1, sin^2 < sin^2(a - b)), its soft band, and beyond (s_v = 0). The
+// flat part runs first without the window's test; from the first height
+// that leaves it, every sample takes the full rule until the window closes.
 __device__ double height_sum(float ell, int num_z, float dz, const SoftWin &v) {
     const float e2 = ell * ell, e3 = e2 * ell;
     double tot = 0.5 * (double)soft_of_sin2(0.f, v);  // z = 0: cos theta = 1, sin theta = 0
     if (e3 == 0.f) return tot;  // ell = 0: cos theta = 0 at every z > 0
-    bool done = false;
-    for (int base = 1; base < num_z && !done; base += kZRun) {
-        const int stop = min(num_z, base + kZRun);
+    int iz = 1;
+    bool flat = true;
+    while (flat && iz < num_z) {  // flat part, runs of kZRun summed in FP32
+        const int stop = min(num_z, iz + kZRun);
         float part = 0.f;
-        for (int iz = base; iz < stop; ++iz) {
+        for (; iz < stop; ++iz) {
             const float z = (float)iz * dz;
-            const float z2 = z * z;
-            const float ih = rsqrtf(e2 + z2);
+            const float ih = rsqrtf(fmaf(z, z, e2));
             const float s = fabsf(z) * ih;  // sin|theta| (z < 0 when the vertical window passes pi/2)
+            if (!(s * s < v.sab2)) {
+                flat = false;  // this height starts the band: not consumed here
+                break;
+            }
+            part = fmaf(e3 * ih, ih * ih, part);
+        }
+        tot += (double)part;
+    }
+    bool done = false;
+    while (!done && iz < num_z) {  // soft band, until the window closes
+        const int stop = min(num_z, iz + kZRun);
+        float part = 0.f;
+        for (; iz < stop; ++iz) {
+            const float z = (float)iz * dz;
+            const float ih = rsqrtf(fmaf(z, z, e2));
+            const float s = fabsf(z) * ih;
             const float s2 = s * s;
             if (s2 > v.sa2) {
                 done = true;
