@@ -8,10 +8,11 @@
 // same linear convolution is evaluated directly:
 //     out[row][m] = scale * sum_j h[m - j] * w[j][v] * in[row][j].
 //
-// B200 layout: a CTA stages R rows (times the weights) and all 2 nu - 1 taps
-// in shared memory with coalesced loads, then each thread produces Q outputs
-// per row (m = t, t+T, ...), reading the weighted row as an R-wide float4
-// broadcast and the taps conflict-free. Pure Ram-Lak taps vanish at even
+// B200 layout: a CTA stages R rows (times the weights; R = 8 while the Q x R
+// accumulators fit, else 4) and all 2 nu - 1 taps in shared memory with
+// coalesced loads, then each thread produces Q outputs per row (m = t, t+T,
+// ...), reading the weighted rows as R/4 float4 broadcasts and the taps
+// conflict-free: each tap read feeds R multiply-adds. Pure Ram-Lak taps vanish at even
 // nonzero offsets (src/aprict/ramp_kernels.py:43-59), so in ODD mode only
 // taps of odd offset are visited plus the centre tap: half the FMAs.
 #include <cuda_runtime.h>
@@ -22,7 +23,7 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kR = 4;  // rows per CTA (float4 of a column)
+constexpr int kR = 4;  // rows per CTA for Q >= 8 (one float4 of a column)
 
 struct RampParams {
     const float *in;
@@ -42,12 +43,13 @@ __device__ __forceinline__ void row_of(const RampParams &P, int64_t r, int &m, i
     v = (int)(r % P.nv);
 }
 
-template <int Q>
+template <int Q, int R>
 __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows) {
+    constexpr int kG = R / 4;  // float4 groups of rows
     extern __shared__ float4 smem4[];
-    float4 *xs = smem4;                                      // [nu] x R rows
-    float *hs = reinterpret_cast<float *>(smem4 + P.nu);     // [2 nu - 1]
-    const int64_t r0 = (int64_t)blockIdx.x * kR;
+    float4 *xs = smem4;                                      // [nu][kG] x 4 rows
+    float *hs = reinterpret_cast<float *>(smem4 + (size_t)P.nu * kG);  // [2 nu - 1]
+    const int64_t r0 = (int64_t)blockIdx.x * R;
     const int nu = P.nu;
 
     for (int k = threadIdx.x; k < 2 * nu - 1; k += kThreads) hs[k] = P.taps[k];
@@ -55,12 +57,12 @@ __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows)
     // (view-major, v fastest): when the v stride is 1 the R rows of one u are
     // adjacent in memory, otherwise each row is contiguous along u.
     float *xf = reinterpret_cast<float *>(xs);
-    const bool v_contig = P.is_v == 1 && P.nv >= kR;
-    for (int e = threadIdx.x; e < kR * nu; e += kThreads) {
+    const bool v_contig = P.is_v == 1 && P.nv >= R;
+    for (int e = threadIdx.x; e < R * nu; e += kThreads) {
         int q, j;
         if (v_contig) {
-            q = e % kR;
-            j = e / kR;
+            q = e % R;
+            j = e / R;
         } else {
             q = e / nu;
             j = e % nu;
@@ -73,15 +75,15 @@ __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows)
             val = P.in[(int64_t)m * P.is_view + (int64_t)j * P.is_u + (int64_t)v * P.is_v];
             if (P.weights) val *= P.weights[(int64_t)j * P.wsu + (int64_t)v * P.wsv];
         }
-        xf[j * kR + q] = val;
+        xf[j * R + q] = val;
     }
     __syncthreads();
 
-    float acc[Q][kR];
+    float acc[Q][R];
 #pragma unroll
     for (int a = 0; a < Q; ++a)
 #pragma unroll
-        for (int q = 0; q < kR; ++q) acc[a][q] = 0.f;
+        for (int q = 0; q < R; ++q) acc[a][q] = 0.f;
 
     const int t = threadIdx.x;
     // Taps index: h[m - j] lives at hs[m - j + nu - 1].
@@ -89,15 +91,20 @@ __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows)
         // m shares the parity of t (kThreads is even); visit j of the other parity.
         const int j0 = 1 - (t & 1);
         for (int j = j0; j < nu; j += 2) {
-            const float4 x = xs[j];
+            float4 x[kG];
+#pragma unroll
+            for (int g = 0; g < kG; ++g) x[g] = xs[j * kG + g];
 #pragma unroll
             for (int a = 0; a < Q; ++a) {
                 const int m = t + a * kThreads;
                 const float h = (m < nu) ? hs[m - j + nu - 1] : 0.f;
-                acc[a][0] = fmaf(h, x.x, acc[a][0]);
-                acc[a][1] = fmaf(h, x.y, acc[a][1]);
-                acc[a][2] = fmaf(h, x.z, acc[a][2]);
-                acc[a][3] = fmaf(h, x.w, acc[a][3]);
+#pragma unroll
+                for (int g = 0; g < kG; ++g) {
+                    acc[a][4 * g + 0] = fmaf(h, x[g].x, acc[a][4 * g + 0]);
+                    acc[a][4 * g + 1] = fmaf(h, x[g].y, acc[a][4 * g + 1]);
+                    acc[a][4 * g + 2] = fmaf(h, x[g].z, acc[a][4 * g + 2]);
+                    acc[a][4 * g + 3] = fmaf(h, x[g].w, acc[a][4 * g + 3]);
+                }
             }
         }
         const float hc = hs[nu - 1];
@@ -105,24 +112,32 @@ __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows)
         for (int a = 0; a < Q; ++a) {
             const int m = t + a * kThreads;
             if (m < nu) {
-                const float4 x = xs[m];
-                acc[a][0] = fmaf(hc, x.x, acc[a][0]);
-                acc[a][1] = fmaf(hc, x.y, acc[a][1]);
-                acc[a][2] = fmaf(hc, x.z, acc[a][2]);
-                acc[a][3] = fmaf(hc, x.w, acc[a][3]);
+#pragma unroll
+                for (int g = 0; g < kG; ++g) {
+                    const float4 x = xs[m * kG + g];
+                    acc[a][4 * g + 0] = fmaf(hc, x.x, acc[a][4 * g + 0]);
+                    acc[a][4 * g + 1] = fmaf(hc, x.y, acc[a][4 * g + 1]);
+                    acc[a][4 * g + 2] = fmaf(hc, x.z, acc[a][4 * g + 2]);
+                    acc[a][4 * g + 3] = fmaf(hc, x.w, acc[a][4 * g + 3]);
+                }
             }
         }
     } else {
         for (int j = 0; j < nu; ++j) {
-            const float4 x = xs[j];
+            float4 x[kG];
+#pragma unroll
+            for (int g = 0; g < kG; ++g) x[g] = xs[j * kG + g];
 #pragma unroll
             for (int a = 0; a < Q; ++a) {
                 const int m = t + a * kThreads;
                 const float h = (m < nu) ? hs[m - j + nu - 1] : 0.f;
-                acc[a][0] = fmaf(h, x.x, acc[a][0]);
-                acc[a][1] = fmaf(h, x.y, acc[a][1]);
-                acc[a][2] = fmaf(h, x.z, acc[a][2]);
-                acc[a][3] = fmaf(h, x.w, acc[a][3]);
+#pragma unroll
+                for (int g = 0; g < kG; ++g) {
+                    acc[a][4 * g + 0] = fmaf(h, x[g].x, acc[a][4 * g + 0]);
+                    acc[a][4 * g + 1] = fmaf(h, x[g].y, acc[a][4 * g + 1]);
+                    acc[a][4 * g + 2] = fmaf(h, x[g].z, acc[a][4 * g + 2]);
+                    acc[a][4 * g + 3] = fmaf(h, x[g].w, acc[a][4 * g + 3]);
+                }
             }
         }
     }
@@ -132,7 +147,7 @@ __global__ void __launch_bounds__(kThreads) k_ramp(RampParams P, int64_t n_rows)
         const int mo = t + a * kThreads;
         if (mo >= nu) continue;
 #pragma unroll
-        for (int q = 0; q < kR; ++q) {
+        for (int q = 0; q < R; ++q) {
             const int64_t r = r0 + q;
             if (r >= n_rows) continue;
             int m, v;
@@ -157,7 +172,10 @@ extern "C" int aprict_b200_ramp_filter(const aprict_proj_desc *in_desc, const fl
     if (taps_dev == nullptr) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ramp filter: null taps");
     if (in_dev == out_dev) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "ramp filter: in-place filtering is not supported");
     const int nu = (int)in_desc->nu;
-    const size_t smem = (size_t)nu * sizeof(float4) + (size_t)(2 * nu - 1) * sizeof(float);
+    const int q = (nu + kThreads - 1) / kThreads;
+    // rows per CTA: 8 while the accumulators fit (Q <= 4), else 4
+    const int rows = q <= 4 ? 8 : kR;
+    const size_t smem = (size_t)nu * rows * sizeof(float) + (size_t)(2 * nu - 1) * sizeof(float);
     if (smem > 200 * 1024) return ab_fail(APRICT_ERR_TOO_LARGE, "ramp filter: nu = %d exceeds shared memory", nu);
     RampParams P;
     P.in = in_dev;
@@ -178,25 +196,24 @@ extern "C" int aprict_b200_ramp_filter(const aprict_proj_desc *in_desc, const fl
     P.scale = scale;
     P.odd = odd_taps_only ? 1 : 0;
     const int64_t n_rows = (int64_t)in_desc->n_views * in_desc->nv;
-    const int64_t blocks = (n_rows + kR - 1) / kR;
+    const int64_t blocks = (n_rows + rows - 1) / rows;
     if (blocks > 0x7fffffff) return ab_fail(APRICT_ERR_TOO_LARGE, "ramp filter: too many rows");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const int q = (nu + kThreads - 1) / kThreads;
-#define AB_RAMP_LAUNCH(QQ)                                                                                    \
+#define AB_RAMP_LAUNCH(QQ, RR)                                                                                \
     do {                                                                                                      \
-        if (smem > 48 * 1024) cudaFuncSetAttribute(k_ramp<QQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        k_ramp<QQ><<<(unsigned)blocks, kThreads, smem, st>>>(P, n_rows);                                      \
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_ramp<QQ, RR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        k_ramp<QQ, RR><<<(unsigned)blocks, kThreads, smem, st>>>(P, n_rows);                                  \
     } while (0)
     if (q <= 1)
-        AB_RAMP_LAUNCH(1);
+        AB_RAMP_LAUNCH(1, 8);
     else if (q <= 2)
-        AB_RAMP_LAUNCH(2);
+        AB_RAMP_LAUNCH(2, 8);
     else if (q <= 4)
-        AB_RAMP_LAUNCH(4);
+        AB_RAMP_LAUNCH(4, 8);
     else if (q <= 8)
-        AB_RAMP_LAUNCH(8);
+        AB_RAMP_LAUNCH(8, 4);
     else if (q <= 16)
-        AB_RAMP_LAUNCH(16);
+        AB_RAMP_LAUNCH(16, 4);
     else
         return ab_fail(APRICT_ERR_TOO_LARGE, "ramp filter: nu = %d exceeds 4096", nu);
 #undef AB_RAMP_LAUNCH
