@@ -1,6 +1,6 @@
 """Siddon forward projector on the GPU vs the FP64 oracle and the reference.
 
-Gate: rel L2 <= 1e-5 against the FP64 oracle (north-star tolerance for
+Gate: rel L2 <= 1e-5 against the FP64 oracle (the stated tolerance for
 projections). Agreement with the reference's own kernel (compiled for the CPU,
 FP32 with incremental stepping) is reported and loosely bounded: the reference
 is the less accurate of the two (its own error vs FP64 is ~5e-6).

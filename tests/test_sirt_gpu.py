@@ -1,6 +1,6 @@
 """SIRT / Landweber on the GPU vs the same iterations composed from FP64 oracle operators.
 
-Gate: rel L2 <= 1e-4 on the reconstruction (north-star tolerance for
+Gate: rel L2 <= 1e-4 on the reconstruction (the stated tolerance for
 reconstructions). The oracle SIRT restates src/aprict/iterators/sirt_vram.py:62-152
 step by step in numpy/FP64.
 """
