@@ -37,7 +37,7 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "SIRT iter/s"
-BASELINE_METRIC = "fwd rays/s, back voxel-updates/s, SIRT iter/s: batched vs plain at rel L2 1e-5"
+HEADLINE_METRIC = "fwd rays/s, back voxel-updates/s, SIRT iter/s: batched vs plain at rel L2 1e-5"
 
 WORKLOADS = {
     "sirt256": dict(
@@ -380,7 +380,7 @@ def run_ours(args) -> dict:
         "data": "synthetic (seeded ellipsoid phantom, simulated Poisson data)",
         "config": {
             "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector, SOD {w['R']} SDD {w['R'] + w['LmR']}",
-            "baseline_metric": BASELINE_METRIC,
+            "baseline_metric": HEADLINE_METRIC,
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "l2": "inputs larger than L2 (b+r 404 MB, x+M 128 MB)",
             "form": "batched: fused residual + all-view backprojection, CUDA-graph replay",
@@ -498,7 +498,7 @@ def run_reference(args) -> dict:
         "data": "synthetic (seeded ellipsoid phantom)",
         "config": {
             "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector",
-            "baseline_metric": BASELINE_METRIC,
+            "baseline_metric": HEADLINE_METRIC,
             "where": "reference device code compiled for the host CPU (oracle/_ref), OpenMP over rays/voxels",
             "oracle_kind": "reference" if oracle.have_ref() else "port",
         },
@@ -635,7 +635,7 @@ def run_batch(args) -> dict:
         "config": {
             "workload": f"batch48: SIRT iteration over {n_scans} scans, edge log-U{w['edge']}, views U{w['views']}, "
                         f"detector U{w['det']}^2, circular/helical with per-view jitter",
-            "baseline_metric": BASELINE_METRIC,
+            "baseline_metric": HEADLINE_METRIC,
             "parallelism": "1 GPU",
             "l2": f"inputs larger than L2 (projections {stats['proj_bytes'] / 1e9:.1f} GB x2)",
             "form": "batched: SIRTBatch, two persistent launches per iteration, CUDA-graph replay",
@@ -688,7 +688,7 @@ def _line(args, metric: str, value: float, unit: str, ms: float, workload: str, 
     out = {
         "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded phantoms)", "config": {"workload": workload, "baseline_metric": BASELINE_METRIC},
+        "data": "synthetic (seeded phantoms)", "config": {"workload": workload, "baseline_metric": HEADLINE_METRIC},
     }
     out.update(extra)
     return out
