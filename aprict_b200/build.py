@@ -7,6 +7,7 @@ rebuild happens only when a source or header is newer than the library.
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import pathlib
 import shutil
@@ -64,20 +65,24 @@ def build(*, force: bool = False, verbose: bool = False, ptxas_verbose: bool = F
         return LIB_PATH
     nvcc = _nvcc()
     BUILD_DIR.mkdir(exist_ok=True)
-    objs = []
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-    for src in sources():
+
+    def compile_one(src: pathlib.Path) -> str:
         obj = BUILD_DIR / (src.stem + ".o")
         cmd = [nvcc, *ARCH_FLAGS, *NVCC_FLAGS, *extra, f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         res = subprocess.run(cmd, capture_output=True, text=True, check=False)
         if res.returncode != 0 or verbose or ptxas_verbose:
-            sys.stderr.write(res.stdout + res.stderr)
+            sys.stderr.write(f"== {src.name}\n" + res.stdout + res.stderr)
         if res.returncode != 0:
             msg = f"nvcc failed on {src.name}"
             raise RuntimeError(msg)
-        objs.append(str(obj))
+        return str(obj)
+
+    # one nvcc per source file, in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(sources()), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(compile_one, sources()))
     tmp = LIB_PATH.with_suffix(".so.tmp")
     cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *objs, "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
     res = subprocess.run(cmd, capture_output=True, text=True, check=False)

@@ -110,7 +110,7 @@ typedef struct {
     float Z_on_val_factor_val;
     uint32_t approx_mode_direct_raycast;
     uint32_t approx_mode_linear_interpolate;
-    uint32_t weighting_preset; /* only 0 is implemented */
+    uint32_t weighting_preset; /* 0 plain, 1-6 cone-cylinder FBP weights, 7 GBC (backproject_gbc) */
     uint32_t ssx, ssy, ssz;
     float soft_vartheta_v, soft_vartheta_v_softspan;
     float soft_vartheta_h, soft_vartheta_h_softspan;
@@ -453,7 +453,9 @@ APRICT_API int aprict_b200_batch_run(const void *plan_host, void *plan_dev, apri
  * per plan, else APRICT_ERR_TOO_LARGE; the first call on each device looks
  * the array up (cudaGetSymbolAddress, which may load the module), so make it
  * before any stream capture; calls that overlap in time on one device share
- * the array and race, so serialise them (one stream, or events). */
+ * the array and race, so serialise them (one stream, or events). After a
+ * device reset the cached address is stale: the next call finds its clearing
+ * memset refused and looks the array up again. */
 APRICT_API int aprict_b200_batch_run_static(const void *plan_host, aprict_stream_t stream);
 
 /* Point-sample compiled shapes onto a grid, "last shape wins"

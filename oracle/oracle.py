@@ -26,7 +26,6 @@ import numpy as np
 HERE = pathlib.Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libaprict_ref.so"
-REF_DIR_DEFAULT = pathlib.Path("/root/reference")
 
 proj_spec = np.dtype(
     {
@@ -69,17 +68,15 @@ class AoBpCfg(ctypes.Structure):
 
 
 def build(ref_dir: pathlib.Path | str | None = None, *, quiet: bool = True) -> None:
-    """Build liboracle.so, and _ref/libaprict_ref.so when the reference sources exist."""
-    ref = pathlib.Path(ref_dir) if ref_dir is not None else REF_DIR_DEFAULT
-    targets = ["liboracle.so"]
-    if (ref / "src/aprict/data/cusrc").is_dir():
-        targets.append("ref")
-    out = subprocess.run(
-        ["make", "-C", str(HERE), f"REF={ref}", *targets],
-        capture_output=True,
-        text=True,
-        check=False,
-    )
+    """Build liboracle.so, and _ref/libaprict_ref.so when the reference sources exist.
+
+    ``ref_dir`` (or the APRICT_REF_DIR environment variable) names the reference
+    checkout; without either, the Makefile's default location is used.
+    """
+    cmd = ["make", "-C", str(HERE), "liboracle.so", "ref-if-present"]
+    if ref_dir is not None:
+        cmd.append(f"REF={ref_dir}")
+    out = subprocess.run(cmd, capture_output=True, text=True, check=False)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

@@ -24,5 +24,5 @@ def _built_libraries() -> None:
     build.build()
     from oracle import oracle
 
-    if not oracle.ORACLE_SO.exists() or (oracle.REF_DIR_DEFAULT.exists() and not oracle.have_ref()):
-        oracle.build()
+    if not oracle.ORACLE_SO.exists() or not oracle.have_ref():
+        oracle.build()  # make: builds what is missing; the reference-compiled part only where its sources exist

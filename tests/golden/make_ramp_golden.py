@@ -7,7 +7,8 @@ and writes ramlak_golden.json: the three (input, expected output) pairs of its
 high-precision values of the linear "same"-mode convolution of the input with
 the Ram-Lak taps of a window 2*len+1, physpixsize 1 (:162-175).
 
-Usage: python tests/golden/make_ramp_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_ramp_golden.py REFERENCE_ROOT
+(or set APRICT_REF_DIR to the reference checkout).
 """
 
 from __future__ import annotations
@@ -17,7 +18,12 @@ import json
 import pathlib
 import sys
 
-REF = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+import os
+
+_ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("APRICT_REF_DIR")
+if not _ref:
+    sys.exit("usage: make_ramp_golden.py REFERENCE_ROOT (or set APRICT_REF_DIR)")
+REF = pathlib.Path(_ref)
 SRC = REF / "src/aprict/tests/ramp_kernels/test_ramp_kernels_precision.py"
 OUT = pathlib.Path(__file__).resolve().parent / "ramlak_golden.json"
 
