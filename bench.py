@@ -379,7 +379,7 @@ def run_ours(args) -> dict:
         "dtype": "f32",
         "data": "synthetic (seeded ellipsoid phantom, simulated Poisson data)",
         "config": {
-            "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector, SOD {w['R']} SDD {w['R'] + w['LmR']}",
+            "workload": workload_text(args.workload, w, M),
             "baseline_metric": HEADLINE_METRIC,
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
             "l2": "inputs larger than L2 (b+r 404 MB, x+M 128 MB)",
@@ -411,10 +411,75 @@ def run_ours(args) -> dict:
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
     }
+    if rank == 0:
+        out["rel_l2_vs_fp64"] = parity_check(pg, x, meas, sirt, w)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_reference(pg, x_true, w, b.cpu().numpy(), sirt)
     replicas.finish()
     return out if rank == 0 else {}
+
+
+def parity_check(pg, x, meas, sirt, w: dict, n_views: int = 8) -> dict:
+    """Relative L2 error of the timed operators against the FP64 oracle, outside the timed region.
+
+    On n_views evenly spaced views of the timed scan and the current iterate x:
+    the forward projection A_s x, and one SIRT update restricted to those views,
+    dx = M (.) B_s(b_s - A_s x), with the same preconditioner M on both sides
+    (the reference's update, src/aprict/iterators/sirt_vram.py:130-152).
+    """
+    import torch
+
+    from aprict_b200.cb import flatpanel as fp
+    from oracle import oracle
+
+    n = w["n"]
+    corner = -np.float32(w["voxwid"]) * np.array((n, n, n), np.float32) / 2
+    sel = np.linspace(0, pg.num_projs, n_views, endpoint=False).astype(int) + 7
+    sel = sel % pg.num_projs
+    pgs = pg.sliced([int(i) for i in sel])
+    specs = pgs.to_proj_spec_array()
+    x_np = x.as_numpy().copy()
+    t0 = time.perf_counter()
+    # forward projection
+    ps = fp.ProjectionSet(pgs, data=None)
+    fp.project(fp.ConfigProject(), x, ps, block=True)
+    want_p, _ = oracle.project_siddon(specs, x_np, voxwid=w["voxwid"], corner=corner)
+    err_fp = _rel_l2(ps.data.cpu().numpy(), want_p)
+    # one SIRT update on the sampled views: residual kernel + backprojection with M
+    b_s = meas.data[torch.as_tensor(sel, device=meas.data.device)].contiguous()
+    r = fp.ProjectionSet(pgs, data=None)
+    fp.project_residual(fp.ConfigProject(multiply_before_adding=-1), x, r, b_s)
+    xn = x.zeroed_copy()
+    fp.backproject(sirt._config_bp, xn, r, summand_multiplier=sirt.preconditioner, block=True)  # noqa: SLF001
+    r_want = b_s.double().cpu().numpy() - want_p
+    mult = sirt.preconditioner.as_numpy().astype(np.float64)
+    dx_want = oracle.backproject(specs, r_want, (n, n, n), sirt._config_bp.contents, voxwid=w["voxwid"],  # noqa: SLF001
+                                 corner=corner, mult=mult)
+    err_res = _rel_l2(r.data.cpu().numpy(), r_want)
+    err_dx = _rel_l2(xn.as_numpy(), dx_want)
+    return {
+        "forward_projection": float(f"{err_fp:.3e}"),
+        "residual": float(f"{err_res:.3e}"),
+        "sirt_update": float(f"{err_dx:.3e}"),
+        "gates": {"projection": 1e-5, "reconstruction": 1e-4},
+        "sample": f"{n_views} of {pg.num_projs} views at full detector and volume size; the update is "
+                  "M (.) B_s(b_s - A_s x) on those views with the iterate x left by the timed steps",
+        "oracle": "FP64 restatement (oracle/ab_oracle.c), OpenMP on the host",
+        "check_s": round(time.perf_counter() - t0, 1),
+    }
+
+
+def _rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def workload_text(name: str, w: dict, n_views: int) -> str:
+    """The workload string both arms print (one text, so both lines name the same configuration)."""
+    return (f"{name}: SIRT iteration, {w['n']}^3 x {w['voxwid']} mm volume, {n_views} views x {w['det']}^2 detector, "
+            f"SOD {w['R']} SDD {w['R'] + w['LmR']}")
 
 
 def cpu_reference(pg, x_true: np.ndarray, w: dict, b: np.ndarray, sirt=None) -> dict:
@@ -437,19 +502,21 @@ def cpu_reference(pg, x_true: np.ndarray, w: dict, b: np.ndarray, sirt=None) -> 
         oracle.ref_project_siddon(specs[sel], x0, voxwid=w["voxwid"], corner=corner, mba=-1.0)
     else:
         oracle.project_siddon(specs[sel], x0, voxwid=w["voxwid"], corner=corner, mba=-1.0)
-    t_fp = (time.perf_counter() - t0) * M / fp_views
+    t_fp_s = time.perf_counter() - t0
+    t_fp = t_fp_s * M / fp_views
     cfg = fp.ConfigBackproject(
         fast_approx=True, cyl_mask_rad=n / 2 * w["voxwid"], apply_summand_multiplier=True, soften_det_edges_proportion=0.05
     )
     mult = np.ones((n, n, n), np.float32)
     vol = np.zeros((n, n, n), np.float32)
-    selb = np.linspace(0, M, bp_views, endpoint=False).astype(int)
+    selb = bp_sample_views(M)
     t0 = time.perf_counter()
     if kind == "reference":
         oracle.ref_backproject(specs[selb], b[selb], vol, cfg.contents, voxwid=w["voxwid"], corner=corner, mult=mult)
     else:
         oracle.backproject(specs[selb], b[selb], (n, n, n), cfg.contents, voxwid=w["voxwid"], corner=corner, mult=mult)
-    t_bp = (time.perf_counter() - t0) * M / bp_views
+    t_bp_s = time.perf_counter() - t0
+    t_bp = t_bp_s * M / bp_views
     t_iter = t_fp + t_bp
     return {
         "value": round(1.0 / t_iter, 6),
@@ -457,7 +524,42 @@ def cpu_reference(pg, x_true: np.ndarray, w: dict, b: np.ndarray, sirt=None) -> 
         "cores": threads,
         "kind": kind,
         "sample": f"projection of {fp_views}/{M} views and backprojection of {bp_views}/{M} views, scaled to the full iteration ({t_fp:.1f} s + {t_bp:.1f} s per iteration)",
+        "sampled_views": {"projection": fp_views, "backprojection": bp_views, "of": M},
+        "sampled_s": round(t_fp_s + t_bp_s, 3),
+        "scale": {"projection": round(M / fp_views, 3), "backprojection": round(M / bp_views, 3)},
     }
+
+
+def bp_sample_views(M: int) -> np.ndarray:
+    """The views the CPU baseline backprojects (evenly spaced)."""
+    bp_views = max(1, min(M, int(os.environ.get("APRICT_CPU_BP_VIEWS", "10"))))
+    return np.linspace(0, M, bp_views, endpoint=False).astype(int)
+
+
+def simulate_data_cpu(pg, x_true: np.ndarray, w: dict, views: np.ndarray) -> np.ndarray:
+    """The measurement b of the GPU arm's recipe on the given views, computed on the host.
+
+    b = -log(Poisson(I0 exp(-A x_true))/I0), capped at log I0, with A the
+    reference's own projector compiled for the CPU; the other views stay zero
+    (the CPU sample never reads them). Same phantom, geometry and photon count
+    as the GPU arm; the Poisson draws come from numpy's generator with the
+    workload's seed.
+    """
+    from oracle import oracle
+
+    n = w["n"]
+    M = pg.num_projs
+    corner = -np.float32(w["voxwid"]) * np.array((n, n, n), np.float32) / 2
+    specs = pg.to_proj_spec_array()[views]
+    if oracle.have_ref():
+        p = oracle.ref_project_siddon(specs, x_true, voxwid=w["voxwid"], corner=corner).astype(np.float64)
+    else:
+        p = oracle.project_siddon(specs, x_true, voxwid=w["voxwid"], corner=corner)[0]
+    rng = np.random.default_rng(w["seed"])
+    counts = np.maximum(rng.poisson(w["photons"] * np.exp(-p)), 1.0)
+    b = np.zeros((M, w["det"], w["det"]), np.float32)
+    b[views] = np.minimum(-np.log(counts / w["photons"]), np.log(w["photons"])).astype(np.float32)
+    return b
 
 
 def run_reference(args) -> dict:
@@ -468,20 +570,22 @@ def run_reference(args) -> dict:
         return {"impl": "reference", "unavailable": "the CPU reference arm is timed on the sirt256 workload only"}
     w = WORKLOADS[args.workload]
     pg, x_true = make_problem(w)
-    n = w["n"]
-    # b from the oracle's own projection of the phantom (no GPU on this arm)
     from oracle import oracle
 
     M = pg.num_projs
-    b = np.zeros((M, w["det"], w["det"]), np.float32)
+    b = simulate_data_cpu(pg, x_true, w, bp_sample_views(M))
     vals = []
+    wall = []
     for _ in range(args.warmup):
         cpu_reference(pg, x_true, w, b)
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         vals.append(cpu_reference(pg, x_true, w, b))
+        wall.append(time.perf_counter() - t0)
     v = statistics.median(c["value"] for c in vals)
-    base = vals[0]
+    base = dict(vals[0])
     base["value"] = v
+    sampled_ms = statistics.median(c["sampled_s"] for c in vals) * 1000.0
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -491,13 +595,23 @@ def run_reference(args) -> dict:
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": round(1000.0 / v, 3),
+        "timing": {
+            "kind": "extrapolated",
+            "what": "each step times the reference's projector on a view sample and its backprojector on another "
+                    "view sample of the full-size iteration; ms_per_step is the time of one whole iteration "
+                    "extrapolated from those samples (per-view cost x views), not a timed whole iteration",
+            "sampled_ms_per_step": round(sampled_ms, 1),
+            "wall_ms_per_step": round(statistics.median(wall) * 1000.0, 1),
+            "sampled_views": base["sampled_views"],
+            "scale": base["scale"],
+        },
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded ellipsoid phantom)",
+        "data": "synthetic (seeded ellipsoid phantom, simulated Poisson data on the sampled views)",
         "config": {
-            "workload": f"{args.workload}: SIRT iteration, {n}^3 x {w['voxwid']} mm volume, {M} views x {w['det']}^2 detector",
+            "workload": workload_text(args.workload, w, M),
             "baseline_metric": HEADLINE_METRIC,
             "where": "reference device code compiled for the host CPU (oracle/_ref), OpenMP over rays/voxels",
             "oracle_kind": "reference" if oracle.have_ref() else "port",
