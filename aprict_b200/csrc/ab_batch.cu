@@ -192,16 +192,20 @@ int with_bp_kernel(int variant, F &&f) {
     }
 }
 
+// Multiprocessor count of the current device, cached per device ordinal (a
+// plan built on another device gets that device's persistent grid).
 int sm_count(int &sms) {
-    static int cached = 0;
-    if (cached == 0) {
-        int dev = 0, n = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+    constexpr int kMaxDev = 64;
+    static int cached[kMaxDev] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return ab_fail(APRICT_ERR_CUDA, "cannot query the current device");
+    int n = (dev >= 0 && dev < kMaxDev) ? __atomic_load_n(&cached[dev], __ATOMIC_RELAXED) : 0;
+    if (n == 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
             return ab_fail(APRICT_ERR_CUDA, "cannot query the multiprocessor count");
-        cached = n;
+        if (dev >= 0 && dev < kMaxDev) __atomic_store_n(&cached[dev], n, __ATOMIC_RELAXED);
     }
-    sms = cached;
+    sms = n;
     return APRICT_OK;
 }
 
@@ -423,17 +427,30 @@ extern "C" int aprict_b200_batch_run_static(const void *plan_host, aprict_stream
     int rc = ab_cuda_check(cudaGetDevice(&dev), "batch_run_static: cudaGetDevice");
     if (rc != APRICT_OK) return rc;
     if (dev < 0 || dev >= kMaxDevices) return ab_fail(APRICT_ERR_TOO_LARGE, "device ordinal %d out of range", dev);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     void *scratch = __atomic_load_n(&g_scratch_addr[dev], __ATOMIC_ACQUIRE);
-    if (scratch == nullptr) {
-        // First call on this device: look up the array's address (this can
-        // load the module, so make the first call before any stream capture).
-        rc = ab_cuda_check(cudaGetSymbolAddress(&scratch, g_batch_scratch), "batch_run_static: cudaGetSymbolAddress");
-        if (rc != APRICT_OK) return rc;
+    cudaError_t e = cudaErrorInvalidValue;
+    // Two tries: a device reset since the address was cached invalidates it,
+    // and the memset then fails; look the array up again once.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        if (scratch == nullptr) {
+            // First call on this device (or after a reset): look up the array's
+            // address (this can load the module, so make the first call before
+            // any stream capture).
+            rc = ab_cuda_check(cudaGetSymbolAddress(&scratch, g_batch_scratch),
+                               "batch_run_static: cudaGetSymbolAddress");
+            if (rc != APRICT_OK) return rc;
+            __atomic_store_n(&g_scratch_addr[dev], scratch, __ATOMIC_RELEASE);
+        }
+        // Counters start at zero for every call, whatever an earlier call left.
+        e = cudaMemsetAsync(scratch, 0, need, st);
+        if (e == cudaSuccess || attempt == 1 || (e != cudaErrorInvalidValue && e != cudaErrorContextIsDestroyed))
+            break;
+        (void)cudaGetLastError();  // the failed memset's (non-sticky) error
+        scratch = nullptr;
         __atomic_store_n(&g_scratch_addr[dev], scratch, __ATOMIC_RELEASE);
     }
-    // Counters start at zero for every call, whatever an earlier call left.
-    rc = ab_cuda_check(cudaMemsetAsync(scratch, 0, need, reinterpret_cast<cudaStream_t>(stream)),
-                       "batch_run_static: clearing the counters");
+    rc = ab_cuda_check(e, "batch_run_static: clearing the counters");
     if (rc != APRICT_OK) return rc;
     return aprict_b200_batch_run(plan_host, scratch, stream);
 }

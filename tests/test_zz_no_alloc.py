@@ -3,8 +3,10 @@ library's static device array (for callers that cannot allocate).
 
 Called through the C ABI and compared with aprict_b200_batch_run on two calls
 in a row (the counters must be clean for the second call), for a projection
-plan and an accumulating backprojection plan; a plan with more launch groups
-than the array holds is rejected before anything is enqueued. This file is
+plan and an accumulating backprojection plan, and for a plan of more than 96
+scans (several launch groups, whose counters sit further into the array); a
+plan with more launch groups than the array holds is rejected before anything
+is enqueued. This file is
 collected last so that it also runs after every other GPU test.
 """
 
@@ -79,6 +81,32 @@ def test_static_scratch_backprojection_matches_batch_run_twice() -> None:
         for va, vb in zip(out_a, out_b):
             assert np.linalg.norm(vb.as_numpy()) > 0
             assert rel_l2(va.as_numpy(), vb.as_numpy()) <= 1e-6, call
+
+
+def test_static_scratch_several_launch_groups_twice() -> None:
+    # 130 small scans = 2 launch groups; each call must start from cleared
+    # counters in both groups' slots (a plan whose counters were left non-zero
+    # by a foreign write would skip work units)
+    rng = np.random.default_rng(34)
+    vols, projs_a, projs_b = [], [], []
+    for i in range(130):
+        n = int(rng.integers(4, 10))
+        vols.append(Volume(rng.random((n, n, n)).astype(np.float32), voxwid=1.0))
+        pg = fp.ProjGeom.new_circular_scan(num_source_points=int(rng.integers(1, 5)), R=40, L_minus_R=40,
+                                           pix_widhei_at_isocenter=(0.7, 0.7), num_pix_widhei=(8, 10),
+                                           theta_start=0.1 * i)
+        projs_a.append(fp.ProjectionSet(pg, data=None))
+        projs_b.append(fp.ProjectionSet(pg, data=None))
+    plan_a = ScanBatch(vols, projs_a).plan_project()
+    plan_b = ScanBatch(vols, projs_b).plan_project()
+    assert plan_a._host[:32].view(np.int32)[4] >= 2  # n_groups
+    for call in range(2):  # accumulating projections: the second call adds the same again
+        _run_static(plan_a)
+        _run_existing(plan_b)
+        torch.cuda.synchronize()
+        for pa, pb in zip(projs_a, projs_b):
+            assert np.linalg.norm(pb.data.cpu().numpy()) > 0
+            assert rel_l2(pa.data.cpu().numpy(), pb.data.cpu().numpy()) <= 1e-6, call
 
 
 def test_static_scratch_rejects_too_many_groups() -> None:
