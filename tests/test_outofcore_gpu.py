@@ -2,10 +2,11 @@
 
 * project_to_array writes exactly what one projection of the whole scan gives
   (bit-identical), for a voxel volume and a FORBILD phantom, with a view count
-  that is not a multiple of the chunk size;
+  that is not a multiple of the chunk size, and matches the FP64 oracle
+  (rel L2 <= 1e-5; the chunked driver of src/aprict/scripts/project_cbfp.py:335-470);
 * with photons_per_pixel the chunks carry Poisson noise of the right size;
 * backproject_from_array equals one all-view backprojection (rel L2 <= 1e-6,
-  chunks summed in order).
+  chunks summed in order) and the FP64 oracle's backprojection (<= 1e-5).
 """
 
 from __future__ import annotations
@@ -18,6 +19,7 @@ from aprict_b200 import FBVolume, Volume, phantoms
 from aprict_b200.cb import flatpanel as fp
 from aprict_b200.outofcore import backproject_from_array, project_to_array
 from helpers import circular, rel_l2
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -30,12 +32,16 @@ def test_project_to_memmap_equals_one_call(tmp_path) -> None:
     out = np.lib.format.open_memmap(tmp_path / "p.npy", "w+", dtype=np.float32, shape=(37, 40, 36))
     assert project_to_array(fp.ConfigProject(), vol, pg, out, views_per_chunk=8) == 0
     np.testing.assert_array_equal(np.asarray(out), one.data.cpu().numpy())
+    want, _ = O.project_siddon(pg.to_proj_spec_array(), vol.as_numpy(), voxwid=1.0,
+                               corner=-np.array((32, 30, 28), np.float32) / 2)
+    assert rel_l2(np.asarray(out), want) <= 1e-5
     fb = FBVolume(phantoms.random_quadric_phantom(3, n_ellipsoids=6, n_cylinders=4, radius=20))
     one = fp.ProjectionSet(pg, data=None)
     fp.project(fp.ConfigProject(), fb, one, block=True)
     out2 = np.zeros((37, 40, 36), np.float32)
     project_to_array(fp.ConfigProject(), fb, pg, out2, views_per_chunk=5)
     np.testing.assert_array_equal(out2, one.data.cpu().numpy())
+    assert rel_l2(out2, O.project_forbild(pg.to_proj_spec_array(), fb.shapes)) <= 1e-5
 
 
 def test_noise() -> None:
@@ -63,3 +69,6 @@ def test_backproject_from_memmap_equals_one_call(tmp_path) -> None:
     backproject_from_array(cfg, b, pg, mm, views_per_chunk=9)
     assert np.linalg.norm(a.as_numpy()) > 0
     assert rel_l2(b.as_numpy(), a.as_numpy()) <= 1e-6
+    want = O.backproject(pg.to_proj_spec_array(), data, (30, 32, 34), cfg.contents, voxwid=1.0,
+                         corner=-np.array((30, 32, 34), np.float32) / 2)
+    assert rel_l2(b.as_numpy(), want) <= 1e-5
