@@ -115,14 +115,20 @@ AB_HD bool ab_siddon_setup(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3]
     const double od[3] = {o.x, o.y, o.z};
     const double dd[3] = {e.x - o.x, e.y - o.y, e.z - o.z};
     double a_in = 0.0, a_out = 1.0;
+    double inv[3];  // 1 / dd (correctly rounded), reused below instead of divisions
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        inv[a] = 0.0;
         if (dd[a] == 0.0) {
             if (!(od[a] > 0.0 && od[a] <= (double)n[a])) return false;
         } else {
-            const double inv = 1.0 / dd[a];
-            const double t0 = (0.0 - od[a]) * inv;
-            const double t1 = ((double)n[a] - od[a]) * inv;
+#if defined(__CUDA_ARCH__)
+            inv[a] = __drcp_rn(dd[a]);
+#else
+            inv[a] = 1.0 / dd[a];
+#endif
+            const double t0 = (0.0 - od[a]) * inv[a];
+            const double t1 = ((double)n[a] - od[a]) * inv[a];
             a_in = fmax(a_in, fmin(t0, t1));
             a_out = fmin(a_out, fmax(t0, t1));
         }
@@ -153,9 +159,9 @@ AB_HD bool ab_siddon_setup(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3]
             const bool pos = dd[a] > 0.0;
             stp[a] = pos ? 1 : -1;
             const double b = pos ? (double)(i + 1) : (double)i;
-            const double ab = (b - od[a]) / dd[a];
+            const double ab = (b - od[a]) * inv[a];
             t0f[a] = (float)((ab - a_in) * len);
-            dtf[a] = (float)(len / fabs(dd[a]));
+            dtf[a] = (float)(len * fabs(inv[a]));
             // Crossings left along this axis until the grid boundary; the last
             // one (k = K-1) is evaluated with the loop's own fma.
             const int K = pos ? n[a] - i : i + 1;
@@ -217,39 +223,81 @@ AB_HD bool ab_siddon(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Visi
     return true;
 }
 
-// Line integral sum(seg * vol[off]) (voxel units), Kahan-compensated, with the
-// gather of the next voxel issued before the current one is accumulated so
-// that one load is always in flight. load(off) must be a pure read.
+// Number of crossings along one axis before the exit: #{k >= 0 : fma(k, dt, t0) < tend},
+// with the traversal's own fma, so the count equals the number of steps the
+// exit test would take along this axis. dt >= 1 (a voxel's chord along an
+// axis is at least its width) keeps the estimate within a few steps of the
+// answer; the two bounded fix-up loops settle it and the final test proves
+// it. ok is cleared when the proof fails (never observed; the caller then
+// takes no steps and reports the ray).
+AB_HD int ab_axis_count(float t0, float dt, float tend, bool &ok) {
+    if (!(t0 < tend)) return 0;  // no crossing before the exit (also t0 = +inf)
+#if defined(__CUDA_ARCH__)
+    const float q = __fdividef(tend - t0, dt);
+#else
+    const float q = (tend - t0) / dt;
+#endif
+    int k = q < 1.f ? 1 : (q > 16777216.f ? 16777216 : (int)ceilf(q));
+    for (int it = 0; it < 8 && k > 1 && fmaf((float)(k - 1), dt, t0) >= tend; ++it) --k;
+    for (int it = 0; it < 8 && fmaf((float)k, dt, t0) < tend; ++it) ++k;
+    if (!(fmaf((float)(k - 1), dt, t0) < tend && fmaf((float)k, dt, t0) >= tend)) ok = false;
+    return k;
+}
+
+// Line integral sum(seg * vol[off]) (voxel units) over the segment o -> e.
+//
+// The loop runs a precomputed number of steps (the crossings before the exit,
+// counted per axis by ab_axis_count), so it needs no exit test per step; each
+// step is the same branch-free advance as ab_siddon. Accumulation is
+// compensated: the products of kChunk consecutive steps are summed in FP32
+// and each partial sum is added to the total with Kahan's compensation (the
+// partial sums carry ~sqrt(kChunk) ulp; the total is then as accurate as a
+// Kahan sum of the partials). load(off) must be a pure read.
 template <typename Off, class Load>
 AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], Load &load, float &sum,
                             bool *bad) {
+    constexpr int kChunk = 16;
     ab_ray<Off> R;
     sum = 0.f;
     if (!ab_siddon_setup<Off>(o, e, n, stride, R, bad)) return false;
+    bool ok = true;
+    const int N = ab_axis_count(R.t0x, R.dtx, R.tend, ok) + ab_axis_count(R.t0y, R.dty, R.tend, ok) +
+                  ab_axis_count(R.t0z, R.dtz, R.tend, ok);
+    if (!ok) {
+        *bad = true;
+        return false;
+    }
     Off off = R.off;
     float kx = 0.f, ky = 0.f, kz = 0.f;
     float tx = R.t0x, ty = R.t0y, tz = R.t0z;
     float t = 0.f, s = 0.f, c = 0.f;
     float mu = load(off);
-    // Unrolled twice (each copy keeps its own exit test): measured 18 % faster
-    // than the plain loop on a 256^3 volume (more independent work per
-    // iteration for the scheduler across the gathers' latency).
-#pragma unroll 2
-    for (;;) {
-        const float tm = fminf(tx, fminf(ty, tz));
-        if (tm >= R.tend) break;
-        const float seg = tm - t;
-        t = tm;
-        AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm);
-        const float mu_next = load(off);  // in the grid: the loop did not stop
-        const float y = seg * mu - c;
+    // Each step: the segment up to the next crossing is accumulated with the
+    // current voxel's value, the crossing is passed, and the next voxel's
+    // value is loaded (in the grid: the step precedes the exit).
+#define AB_GATHER_STEP(part)                                   \
+    do {                                                       \
+        const float tm_ = fminf(tx, fminf(ty, tz));            \
+        part = fmaf(tm_ - t, mu, part);                        \
+        t = tm_;                                               \
+        AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm_); \
+        mu = load(off);                                        \
+    } while (0)
+    int i = 0;
+    for (; i + kChunk <= N; i += kChunk) {
+        float part = 0.f;
+#pragma unroll
+        for (int j = 0; j < kChunk; ++j) AB_GATHER_STEP(part);
+        const float y = part - c;
         const float tt = s + y;
         c = (tt - s) - y;
         s = tt;
-        mu = mu_next;
     }
-    s += (R.tend - t) * mu - c;  // the last segment ends at the exit
-    sum = s;
+    float part = 0.f;
+    for (; i < N; ++i) AB_GATHER_STEP(part);
+#undef AB_GATHER_STEP
+    part = fmaf(R.tend - t, mu, part);  // the last segment ends at the exit
+    sum = s + (part - c);
     return true;
 }
 

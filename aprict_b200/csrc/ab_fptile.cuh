@@ -28,8 +28,16 @@ struct TileMap {
     int tile_w, tile_u, tile_v;  // tile extents: views, pixels along u, pixels along v
     int warp_w, warp_u, warp_v;  // a warp's patch (product 32)
     int ntw, ntu, ntv;           // number of tiles along views, u, v
+    // log2 of the power-of-two extents above, for shift/mask decomposition
+    int lg_warp_u, lg_warp_v, lg_nwu, lg_nwv, lg_tile_u;
     uint64_t units() const { return (uint64_t)ntw * ntu * ntv; }
 };
+
+inline int ilog2_pow2(int x) {
+    int l = 0;
+    while ((1 << l) < x) ++l;
+    return l;
+}
 
 // Tile shapes: tv == 1 -> one detector row per tile (used when nv < 8);
 // otherwise warps are 1 (view) x 4 (u) x 8 (v) patches of a 4 x 4 x 16
@@ -60,6 +68,11 @@ inline TileMap make_tiles(uint32_t nu, uint32_t nv, uint32_t n_views) {
     }
     t.warp_u = 32 / (t.warp_w * t.warp_v);
     t.tile_u = kThreads / (t.tile_w * t.tile_v);
+    t.lg_warp_u = ilog2_pow2(t.warp_u);
+    t.lg_warp_v = ilog2_pow2(t.warp_v);
+    t.lg_nwu = ilog2_pow2(t.tile_u / t.warp_u);
+    t.lg_nwv = ilog2_pow2(t.tile_v / t.warp_v);
+    t.lg_tile_u = ilog2_pow2(t.tile_u);
     t.ntu = (int)((nu + t.tile_u - 1) / t.tile_u);
     t.ntv = (int)((nv + t.tile_v - 1) / t.tile_v);
     t.ntw = (int)((n_views + t.tile_w - 1) / t.tile_w);
@@ -70,28 +83,41 @@ inline TileMap make_tiles(uint32_t nu, uint32_t nv, uint32_t n_views) {
 // band slowest: the CTAs resident at one time work on one band of rows of
 // some tens of views, whose rays cross only a slab of the volume, so the
 // volume data they gather stays in L2 (rather than whole views, which touch
-// all of it). False when the thread has no ray (past the last view).
+// all of it). tile_thread maps (column tile tu, view group tw, row band tv)
+// and the thread to its ray; every extent inside a tile is a power of two, so
+// the decomposition is shifts and masks. False when the thread has no ray
+// (past the last view).
+__device__ __forceinline__ bool tile_thread(const TileMap &tm, uint32_t n_views, int tu, int tw, int tv, int &view,
+                                            int &iu, int &iv) {
+    const int t = threadIdx.x;
+    if (tm.tile_v == 1) {
+        view = tw;
+        iu = (tu << tm.lg_tile_u) + t;
+        iv = tv;
+    } else {
+        const int lane = t & 31, warp = t >> 5;
+        const int lv = lane & (tm.warp_v - 1);
+        const int lu = (lane >> tm.lg_warp_v) & (tm.warp_u - 1);
+        const int lw = lane >> (tm.lg_warp_v + tm.lg_warp_u);
+        const int wv = warp & ((1 << tm.lg_nwv) - 1);
+        const int wu = (warp >> tm.lg_nwv) & ((1 << tm.lg_nwu) - 1);
+        const int ww = warp >> (tm.lg_nwv + tm.lg_nwu);
+        view = tw * tm.tile_w + ww * tm.warp_w + lw;
+        iu = (tu << tm.lg_tile_u) + (wu << tm.lg_warp_u) + lu;
+        iv = tv * tm.tile_v + (wv << tm.lg_warp_v) + lv;
+    }
+    return view < (int)n_views;
+}
+
+// The same for a linear work-unit index b (column tile fastest, then view
+// group, then row band).
 __device__ __forceinline__ bool block_tile(const TileMap &tm, uint32_t n_views, uint32_t b, int &view, int &iu,
                                            int &iv) {
     const int tu = (int)(b % (uint32_t)tm.ntu);
     const uint32_t rest = b / (uint32_t)tm.ntu;
     const int tw = (int)(rest % (uint32_t)tm.ntw);
     const int tv = (int)(rest / (uint32_t)tm.ntw);
-    const int t = threadIdx.x;
-    if (tm.tile_v == 1) {
-        view = tw;
-        iu = tu * tm.tile_u + t;
-        iv = tv;
-    } else {
-        const int lane = t & 31, warp = t >> 5;
-        const int lv = lane % tm.warp_v, lu = (lane / tm.warp_v) % tm.warp_u, lw = lane / (tm.warp_v * tm.warp_u);
-        const int nwv = tm.tile_v / tm.warp_v, nwu = tm.tile_u / tm.warp_u;
-        const int wv = warp % nwv, wu = (warp / nwv) % nwu, ww = warp / (nwv * nwu);
-        view = tw * tm.tile_w + ww * tm.warp_w + lw;
-        iu = tu * tm.tile_u + wu * tm.warp_u + lu;
-        iv = tv * tm.tile_v + wv * tm.warp_v + lv;
-    }
-    return view < (int)n_views;
+    return tile_thread(tm, n_views, tu, tw, tv, view, iu, iv);
 }
 
 // L2 policy for the volume gathers: keep the volume resident (evict_last)
@@ -138,9 +164,7 @@ struct FPScan {
 // calls it with the same b. No barriers inside. SS1: one sub-ray per pixel
 // (ssu = ssv = 1), which keeps nothing but the sum live across the traversal.
 template <typename Off, bool SS1>
-__device__ __forceinline__ void fp_tile(const FPScan<Off> &S, uint32_t b) {
-    int view, iu, iv;
-    if (!block_tile(S.tm, S.n_views, b, view, iu, iv) || iu >= (int)S.nu || iv >= (int)S.nv) return;
+__device__ __forceinline__ void fp_ray(const FPScan<Off> &S, int view, int iu, int iv) {
     const uint64_t pol = l2_evict_last_policy();
     bool bad = false;
     float tot;
@@ -182,6 +206,14 @@ __device__ __forceinline__ void fp_tile(const FPScan<Off> &S, uint32_t b) {
     } else {
         atomicAdd(S.out + o, tot);
     }
+}
+
+// Rays of work unit b (linear tile order) of scan S.
+template <typename Off, bool SS1>
+__device__ __forceinline__ void fp_tile(const FPScan<Off> &S, uint32_t b) {
+    int view, iu, iv;
+    if (!block_tile(S.tm, S.n_views, b, view, iu, iv) || iu >= (int)S.nu || iv >= (int)S.nv) return;
+    fp_ray<Off, SS1>(S, view, iu, iv);
 }
 
 // Host: argument checks shared by the projector and its adjoint.

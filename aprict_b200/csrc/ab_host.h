@@ -27,7 +27,8 @@ enum {
     AB_TUNE_FP_WARP_V = 3,  // forward projector lanes of a warp along v (0 = auto = 8, 8, 16, 32)
     AB_TUNE_FP_VIEWS = 4,   // forward projector views per tile (0 = auto = 4, 1, 2, 4)
     AB_TUNE_FP_WARP_VIEWS = 5,  // forward projector views inside a warp's patch (0 = auto = 1, 1, 2, 4)
-    AB_TUNE_COUNT = 6
+    AB_TUNE_FP_SS1 = 6,     // one-scan projector, one sub-ray per pixel: 0 = specialised path, 1 = general path
+    AB_TUNE_COUNT = 7
 };
 int ab_tuning_get(int key);
 

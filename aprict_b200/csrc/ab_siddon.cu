@@ -17,13 +17,43 @@ struct ScatterVisit {
     }
 };
 
-// The one-scan kernel always takes the general sub-ray path: with the scan
-// in the constant bank it measured 6 % faster than the single-sub-ray
-// specialisation on a 256^3 volume (the batch kernel, which indexes its scans'
-// parameters, is 16 % faster with the specialisation).
+// Projector kernels over linear tile indices (used when the tile counts do
+// not fit a 3-D grid).
 template <typename Off, bool SS1>
 __global__ void __launch_bounds__(kThreads, 4) k_project_siddon(const FPScan<Off> S) {
     fp_tile<Off, SS1>(S, blockIdx.x);
+}
+
+// The same with the tile given by a 3-D grid (x: column tile, y: view group,
+// z: row band; the hardware issues blocks in that linear order), which saves
+// the per-thread division of a linear block index. With one sub-ray per pixel
+// the specialised ray path runs (no spills; 12.35 ms against 13.25 ms for the
+// general path on the 256^3 x 360-view fused residual, bit-identical results);
+// tuning knob 6 = 1 forces the general path.
+template <typename Off, bool SS1>
+__global__ void __launch_bounds__(kThreads, 4) k_project_siddon_3d(const FPScan<Off> S) {
+    int view, iu, iv;
+    if (!tile_thread(S.tm, S.n_views, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, view, iu, iv) ||
+        iu >= (int)S.nu || iv >= (int)S.nv)
+        return;
+    fp_ray<Off, SS1>(S, view, iu, iv);
+}
+
+template <typename Off>
+int launch_project(const FPScan<Off> &S, uint64_t nblocks, cudaStream_t st) {
+    const TileMap &tm = S.tm;
+    const bool ss1 = S.ssu == 1 && S.ssv == 1;
+    if (tm.ntw <= 65535 && tm.ntv <= 65535 && tm.ntu <= 0x7fffffff) {
+        const dim3 grid((unsigned)tm.ntu, (unsigned)tm.ntw, (unsigned)tm.ntv);
+        if (ss1 && ab_tuning_get(AB_TUNE_FP_SS1) == 0)
+            k_project_siddon_3d<Off, true><<<grid, kThreads, 0, st>>>(S);
+        else
+            k_project_siddon_3d<Off, false><<<grid, kThreads, 0, st>>>(S);
+    } else {
+        if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
+        k_project_siddon<Off, false><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
+    }
+    return APRICT_OK;
 }
 
 template <typename Off>
@@ -68,15 +98,14 @@ extern "C" int aprict_b200_project_siddon(const aprict_proj_spec *specs_dev, con
         const FPScan<int32_t> S =
             make_fpscan<int32_t>(specs_dev, pd, projs_dev, base_dev, vd, vol_dev, cfg, status_dev, nblocks);
         if (nblocks == 0) return APRICT_OK;
-        if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
-        k_project_siddon<int32_t, false><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
+        rc = launch_project<int32_t>(S, nblocks, st);
     } else {
         const FPScan<int64_t> S =
             make_fpscan<int64_t>(specs_dev, pd, projs_dev, base_dev, vd, vol_dev, cfg, status_dev, nblocks);
         if (nblocks == 0) return APRICT_OK;
-        if (nblocks > 0x7fffffffull) return ab_fail(APRICT_ERR_TOO_LARGE, "too many detector tiles");
-        k_project_siddon<int64_t, false><<<(unsigned)nblocks, kThreads, 0, st>>>(S);
+        rc = launch_project<int64_t>(S, nblocks, st);
     }
+    if (rc != APRICT_OK) return rc;
     return ab_cuda_check(cudaGetLastError(), "project_siddon launch");
 }
 

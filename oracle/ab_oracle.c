@@ -329,6 +329,47 @@ static int masked(const ao_grid *g, const ao_bp_cfg *c, int ix, int iy, int iz) 
     return x.x * x.x + x.y * x.y > c->mask_rad * c->mask_rad;
 }
 
+/* Nearest-pixel choices that FP64 cannot settle: per voxel, the number of
+ * (sub-sample, view) pairs of the fast nearest mode whose detector coordinate
+ * (fu or fv, in pixel indices, inside the detector) lies within eps of a
+ * half-integer, where floor(f + 1/2) flips with the rounding of the
+ * coordinate's evaluation. Symmetric geometries make them exact in real
+ * arithmetic (voxel centres projecting onto pixel boundaries); any two FP64
+ * evaluations may then pick different neighbours. */
+void ao_bp_nearest_ties(const ao_proj_spec *specs, int n_views, const ao_grid *g, const ao_bp_cfg *c, double eps,
+                        int32_t *counts, int nthreads) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for collapse(2) schedule(dynamic, 2)
+    for (int ix = 0; ix < g->nx; ++ix) {
+        for (int iy = 0; iy < g->ny; ++iy) {
+            for (int iz = 0; iz < g->nz; ++iz) {
+                const int64_t o = vidx(g, ix, iy, iz);
+                counts[o] = 0;
+                if (masked(g, c, ix, iy, iz)) continue;
+                const d3 xc = voxel_centre(g, ix, iy, iz);
+                int cnt = 0;
+                for (int si = 0; si < c->ssx; ++si)
+                    for (int sj = 0; sj < c->ssy; ++sj)
+                        for (int sk = 0; sk < c->ssz; ++sk) {
+                            const d3 x = add(xc, scl((d3){-0.5 + (si + 0.5) / c->ssx, -0.5 + (sj + 0.5) / c->ssy,
+                                                          -0.5 + (sk + 0.5) / c->ssz},
+                                                     g->voxwid));
+                            for (int m = 0; m < n_views; ++m) {
+                                const int nu = (int)specs[m].nu, nv = (int)specs[m].nv;
+                                double cu, cv;
+                                det_coords(&specs[m], x, &cu, &cv);
+                                const double fu = cu + (nu - 1) / 2.0, fv = cv + (nv - 1) / 2.0;
+                                if (!(fu > -1.0 && fu < nu && fv > -1.0 && fv < nv)) continue;
+                                const double du = fabs(fu - floor(fu) - 0.5), dv = fabs(fv - floor(fv) - 0.5);
+                                if (du < eps || dv < eps) ++cnt;
+                            }
+                        }
+                counts[o] = cnt;
+            }
+        }
+    }
+}
+
 void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
                     const ao_grid *g, const double *mult, const ao_bp_cfg *c, double *vol, int nthreads) {
     const int64_t nvox = (int64_t)g->nx * g->ny * g->nz;

@@ -47,6 +47,9 @@ void ao_backproject_transpose(const ao_proj_spec *specs, int n_views, int nu, in
 
 /* vol += mult * BP(projs), the voxel-driven backprojector of
  * _backproject_CB_getval (CB_backproject.cu:313-733), presets 0-6, in FP64. */
+/* Per voxel: fast-nearest (sub-sample, view) pairs whose pixel choice lies within eps of a tie. */
+void ao_bp_nearest_ties(const ao_proj_spec *specs, int n_views, const ao_grid *g, const ao_bp_cfg *c, double eps,
+                        int32_t *counts, int nthreads);
 void ao_backproject(const ao_proj_spec *specs, int n_views, int nu, int nv, const double *projs,
                     const ao_grid *g, const double *mult, const ao_bp_cfg *cfg, double *vol, int nthreads);
 

@@ -234,6 +234,29 @@ def backproject(
     return out
 
 
+def bp_nearest_ties(
+    specs: np.ndarray,
+    shape: tuple[int, int, int],
+    cfg_contents: np.ndarray,
+    *,
+    voxwid: float,
+    corner: np.ndarray,
+    order: str = "C",
+    eps: float = 1e-9,
+    nthreads: int | None = None,
+) -> np.ndarray:
+    """Per voxel, the number of fast-nearest (sub-sample, view) pairs whose pixel choice
+    lies within eps pixel of a half-integer tie (FP64 cannot settle those)."""
+    lib = _load(ORACLE_SO)
+    s = _specs(specs)
+    out = np.zeros(shape, dtype=np.int32, order=order)
+    g = grid(shape, voxwid, corner, order)
+    k = bp_cfg_from_contents(cfg_contents)
+    lib.ao_bp_nearest_ties(_p(s), len(s), ctypes.byref(g), ctypes.byref(k), ctypes.c_double(eps), _p(out),
+                           nthreads or nthreads_default())
+    return out
+
+
 # ------------------------------------------------------- reference compiled for the CPU
 def ref_project_siddon(
     specs: np.ndarray,
