@@ -20,7 +20,7 @@ from . import _lib
 from .cb import flatpanel as fp
 from .volume import Volume
 
-KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V, KEY_FP_VIEWS, KEY_FP_WARP_VIEWS, KEY_FP_SS1 = 0, 1, 2, 3, 4, 5, 6
+KEY_FP_TILE_V, KEY_BP_XB, KEY_BP_WAVE, KEY_FP_WARP_V, KEY_FP_VIEWS, KEY_FP_WARP_VIEWS, KEY_FP_SS1, KEY_BP_ZLANES = range(8)
 FP_TILE_V = (8, 16, 32)
 FP_WARP_V = (8, 16, 32)
 FP_VIEWS = ((1, 1), (2, 1), (2, 2), (4, 1), (4, 2))  # (views per tile, views inside a warp)
@@ -46,6 +46,7 @@ def current() -> dict:
         "bp_xb": lib.aprict_b200_get_tuning(KEY_BP_XB),
         "bp_wave": lib.aprict_b200_get_tuning(KEY_BP_WAVE),
         "fp_ss1": lib.aprict_b200_get_tuning(KEY_FP_SS1),
+        "bp_zlanes": lib.aprict_b200_get_tuning(KEY_BP_ZLANES),
     }
 
 
@@ -58,6 +59,7 @@ def apply(choice: dict) -> None:
     _set(KEY_BP_XB, choice.get("bp_xb", 0))
     _set(KEY_BP_WAVE, choice.get("bp_wave", 0))
     _set(KEY_FP_SS1, choice.get("fp_ss1", 0))
+    _set(KEY_BP_ZLANES, choice.get("bp_zlanes", 0))
 
 
 def _time(fn, reps: int = 3) -> float:

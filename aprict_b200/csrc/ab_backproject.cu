@@ -40,15 +40,22 @@ extern "C" int aprict_b200_backproject(const aprict_proj_spec *specs_dev, const 
     BPParams P;
     uint64_t grid = 0;
     int xb = 2;
+    int ord = 0;
     // Slice stacks (one z layer) always take two voxels per thread.
     const int rc = make_bp_params(specs_dev, pd, projs_dev, vd, vol_dev, multiplier_dev, cfg, status_dev, P, grid, xb,
-                                  vd != nullptr && bp_ord(vd) == 2 ? 2 : 0);
+                                  vd != nullptr && bp_ord(vd) == 2 ? 2 : 0, &ord);
     if (rc != APRICT_OK || grid == 0) return rc;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const bool lin = cfg->approx_mode_linear_interpolate != 0;
-    const int ord = bp_ord(vd);
     if (ord == 2) {
-        launch_bp<2, 2>(P, cfg, lin, (unsigned)grid, st);  // slices (xb forced to 2 below)
+        launch_bp<2, 2>(P, cfg, lin, (unsigned)grid, st);  // slices (xb forced to 2 above)
+    } else if (ord == 3) {  // C order, z columns
+        if (xb == 8)
+            launch_bp<3, 8>(P, cfg, lin, (unsigned)grid, st);
+        else if (xb == 4)
+            launch_bp<3, 4>(P, cfg, lin, (unsigned)grid, st);
+        else
+            launch_bp<3, 2>(P, cfg, lin, (unsigned)grid, st);
     } else if (xb == 8) {
         if (ord == 0)
             launch_bp<0, 8>(P, cfg, lin, (unsigned)grid, st);

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb
 
 // Backprojection kernel variant code: ORD + 3 * mode (ORD from ab_bp::bp_ord),
 // mode 0 fast nearest, 1 fast bilinear, 2 raycast nearest, 3 raycast
-// bilinear, 4 exact.
+// bilinear, 4 exact; 15: fast nearest in the z-column layout (ORD 3).
 int bp_variant(const aprict_backproject_config *c, const aprict_vol_desc *vd) {
     const int mode = c->exact ? 4
                               : (c->approx_mode_direct_raycast ? 2 : 0) + (c->approx_mode_linear_interpolate ? 1 : 0);
@@ -166,7 +166,7 @@ int bp_variant(const aprict_backproject_config *c, const aprict_vol_desc *vd) {
 // The batch backprojection kernel of a variant code.
 template <int V>
 auto bp_kernel() {
-    constexpr int ORD = V % 3, mode = V / 3;
+    constexpr int ORD = V == 15 ? 3 : V % 3, mode = V == 15 ? 0 : V / 3;
     return k_batch_backproject<ORD, mode == 4, mode == 2 || mode == 3, mode == 1 || mode == 3>;
 }
 
@@ -188,6 +188,7 @@ int with_bp_kernel(int variant, F &&f) {
         case 12: return f(bp_kernel<12>());
         case 13: return f(bp_kernel<13>());
         case 14: return f(bp_kernel<14>());
+        case 15: return f(bp_kernel<15>());
         default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", variant);
     }
 }
@@ -272,6 +273,15 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
     std::vector<ab_bp::BPParams> bp(op == APRICT_BATCH_BACKPROJECT ? n_scans : 0);
     bool all_small = true, all_ss1 = true;
     int variant = -1;
+    // The z-column layout for a backprojection batch only when every scan
+    // qualifies (one kernel variant per plan; each scan then gets the layout
+    // its one-scan call would take).
+    bool zlanes = op == APRICT_BATCH_BACKPROJECT && n_scans > 0;
+    for (int i = 0; zlanes && i < n_scans; ++i) {
+        const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
+        const int xb = batch_xb(ab_bp::bp_ord(&scans[i].vol), cfg->exact != 0);
+        zlanes = ab_bp::bp_zlanes_ok(&scans[i].vol, xb, cfg) && batch_xb(3, cfg->exact != 0) == xb;
+    }
     for (int i = 0; i < n_scans; ++i) {
         const aprict_scan &sc = scans[i];
         int rc;
@@ -289,12 +299,13 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             units[i] = u;
         } else {
             const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
-            int xb = 0;
+            int xb = 0, ord = -1;
             uint64_t u = 0;
             rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
-                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol), cfg->exact != 0));
+                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol), cfg->exact != 0),
+                                       zlanes ? &ord : nullptr);
             if (rc != APRICT_OK) return scan_error(rc, i);
-            const int v = bp_variant(cfg, &sc.vol);
+            const int v = ord == 3 ? 15 : bp_variant(cfg, &sc.vol);
             if (variant >= 0 && v != variant)
                 return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
                                "scan %d: every scan of a backprojection batch needs the same volume order, "

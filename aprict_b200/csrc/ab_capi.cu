@@ -16,7 +16,7 @@ static_assert(sizeof(aprict_scan) == 120 && offsetof(aprict_scan, vol) == 64 && 
               "scan layout");
 
 static thread_local char g_last_error[512] = "";
-static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0, 0, 0, 0, 0};
+static int g_tuning[AB_TUNE_COUNT] = {0, 0, 0, 0, 0, 0, 0, 0};
 
 int ab_tuning_get(int key) { return key >= 0 && key < AB_TUNE_COUNT ? __atomic_load_n(&g_tuning[key], __ATOMIC_RELAXED) : 0; }
 
@@ -105,7 +105,8 @@ int aprict_b200_set_tuning(int key, int value) {
         case AB_TUNE_FP_WARP_V: ok = value == 0 || value == 8 || value == 16 || value == 32; break;
         case AB_TUNE_FP_VIEWS:
         case AB_TUNE_FP_WARP_VIEWS: ok = value == 0 || value == 1 || value == 2 || value == 4; break;
-        case AB_TUNE_FP_SS1: ok = value == 0 || value == 1; break;
+        case AB_TUNE_FP_SS1:
+        case AB_TUNE_BP_ZLANES: ok = value == 0 || value == 1; break;
         default: ok = value >= 0 && value <= 16; break;
     }
     if (!ok) return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "tuning value %d not allowed for key %d", value, key);

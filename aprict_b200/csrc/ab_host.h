@@ -28,7 +28,8 @@ enum {
     AB_TUNE_FP_VIEWS = 4,   // forward projector views per tile (0 = auto = 4, 1, 2, 4)
     AB_TUNE_FP_WARP_VIEWS = 5,  // forward projector views inside a warp's patch (0 = auto = 1, 1, 2, 4)
     AB_TUNE_FP_SS1 = 6,     // one-scan projector, one sub-ray per pixel: 0 = specialised path, 1 = general path
-    AB_TUNE_COUNT = 7
+    AB_TUNE_BP_ZLANES = 7,  // one-scan backprojector on C-order volumes: 0 = z-column layout when tall enough, 1 = never
+    AB_TUNE_COUNT = 8
 };
 int ab_tuning_get(int key);
 

@@ -411,6 +411,27 @@ def run_ours(args) -> dict:
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
     }
+    if not args.no_batch48 and args.workload == "sirt256":
+        # the batched uneven-scan workload at its full ranges, a few iterations
+        t0 = time.perf_counter()
+        wb = WORKLOADS["batch48"]
+        rb = batch48_measure(wb, steps=3, warmup=2, local=local, k_plain=2)
+        out["components"]["batch48"] = {
+            "workload": f"48 scans, edge log-U{wb['edge']}, views U{wb['views']}, detector U{wb['det']}^2, "
+                        "circular/helical with per-view jitter; one SIRT iteration of all scans per step",
+            "batched_ms_per_step": round(rb["ms"], 3),
+            "per_scan_launch_ms_per_step": round(rb["ms_per_scan"], 3),
+            "reference_pattern_ms_per_step": round(rb["ms_ref_pattern"], 3),
+            "batched_over_per_scan": round(rb["ms_per_scan"] / rb["ms"], 3),
+            "batched_over_reference_pattern": round(rb["ms_ref_pattern"] / rb["ms"], 3),
+            "batched_fp_ms": round(rb["t_fp_batch"], 3),
+            "batched_bp_ms": round(rb["t_bp_batch"], 3),
+            "fwd_rays_per_s": round(rb["stats"]["rays"] / (rb["t_fp_batch"] * 1e-3), 1),
+            "back_voxel_updates_per_s": round(rb["stats"]["voxel_views"] / (rb["t_bp_batch"] * 1e-3), 1),
+            "steps": 3,
+            "section_s": round(time.perf_counter() - t0, 1),
+        }
+        out["gpu_launches_batch48"] = 2 * 3
     if rank == 0:
         out["rel_l2_vs_fp64"] = parity_check(pg, x, meas, sirt, w)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -621,16 +642,11 @@ def run_reference(args) -> dict:
     }
 
 
-def run_batch(args) -> dict:
-    """Workload batch48: SIRT over 48 uneven scans, batched vs plain launches.
-
-    A step is one SIRT iteration of all 48 scans. ``value`` is the batched
-    form (SIRTBatch: two persistent launches per iteration, replayed from a
-    CUDA graph). Beside it: the same kernels launched per scan (fused residual
-    + all-view backprojection, 96 launches per iteration) and the reference's
-    launch pattern per scan (copy, accumulate projection, 10-view
-    backprojection launches, a host synchronisation per scan).
-    """
+def batch48_measure(w: dict, steps: int, warmup: int, local: int, k_plain: int | None = None) -> dict:
+    """SIRT over the 48 uneven scans of workload w: batched (graph-replayed
+    SIRTBatch) against per-scan launches of the same kernels and against the
+    reference's launch pattern. Returns the timings (ms per iteration of all
+    scans), the batched component kernels and the workload's sizes."""
     import torch
 
     from aprict_b200 import Volume, geometry, phantoms
@@ -638,9 +654,6 @@ def run_batch(args) -> dict:
     from aprict_b200.cb import flatpanel as fp
     from aprict_b200.iterators import SIRT_flatpanel, SIRTBatch
 
-    rank, world, local = _env_rank()
-    torch.cuda.set_device(local)
-    w = WORKLOADS[args.workload]
     rng = np.random.default_rng(w["seed"])
     params = geometry.uneven_scans(rng, w["n_scans"], edge=w["edge"], views=w["views"], det=w["det"],
                                    voxwid=w["voxwid"], R=w["R"], L_minus_R=w["LmR"])
@@ -693,10 +706,10 @@ def run_batch(args) -> dict:
     # batched SIRT (graph replay), the headline
     sb = SIRTBatch(sirts)
     sb.iterate_graph(1)
-    for _ in range(max(0, args.warmup - 1)):
+    for _ in range(max(0, warmup - 1)):
         sb.iterate_graph(1)
     with ClockSampler(local) as clk:
-        ms = timed(lambda: sb.iterate_graph(1), args.steps)
+        ms = timed(lambda: sb.iterate_graph(1), steps)
 
     # per-scan launches of the same kernels (no host synchronisation)
     cfg_res = fp.ConfigProject(multiply_before_adding=-1)
@@ -706,7 +719,7 @@ def run_batch(args) -> dict:
             s.iterate()
 
     per_scan_iter()
-    k_plain = max(2, args.steps // 2)
+    k_plain = k_plain or max(2, steps // 2)
     ms_per_scan = timed(per_scan_iter, k_plain)
 
     # the reference's launch pattern per scan
@@ -731,8 +744,29 @@ def run_batch(args) -> dict:
     ms_ref_pattern = timed(ref_pattern_iter, k_plain)
     del cfg_res
 
+    return dict(ms=ms, ms_per_scan=ms_per_scan, ms_ref_pattern=ms_ref_pattern, t_fp_batch=t_fp_batch,
+                t_bp_batch=t_bp_batch, stats=stats, n_scans=len(sirts), clocks=clk.summary())
+
+
+def run_batch(args) -> dict:
+    """Workload batch48: SIRT over 48 uneven scans, batched vs plain launches.
+
+    A step is one SIRT iteration of all 48 scans. ``value`` is the batched
+    form (SIRTBatch: two persistent launches per iteration, replayed from a
+    CUDA graph). Beside it: the same kernels launched per scan (fused residual
+    + all-view backprojection, 96 launches per iteration) and the reference's
+    launch pattern per scan (copy, accumulate projection, 10-view
+    backprojection launches, a host synchronisation per scan).
+    """
+    import torch
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    r = batch48_measure(w, args.steps, args.warmup, local)
+    ms, ms_per_scan, ms_ref_pattern = r["ms"], r["ms_per_scan"], r["ms_ref_pattern"]
+    t_fp_batch, t_bp_batch, stats, n_scans = r["t_fp_batch"], r["t_bp_batch"], r["stats"], r["n_scans"]
     peak, peak_kind = load_peaks()
-    n_scans = len(sirts)
     out = {
         "metric": "batched SIRT iter/s (48 uneven scans per iteration)",
         "value": round(1000.0 / ms, 4),
@@ -779,7 +813,7 @@ def run_batch(args) -> dict:
         },
         "e2e": None,
         "gpu_launches": 2 * args.steps,
-        "clocks": clk.summary(),
+        "clocks": r["clocks"],
     }
     return out if rank == 0 else {}
 
@@ -806,6 +840,59 @@ def _line(args, metric: str, value: float, unit: str, ms: float, workload: str, 
     }
     out.update(extra)
     return out
+
+
+def quadric_tests(pg, shapes: np.ndarray, tile: int = 16) -> tuple[int, int]:
+    """Ray-shape tests of the analytic projector after its tile cull, and their FP64 FLOPs.
+
+    The cull restated on the host: per view, each shape's world bounding box
+    (8 corners, from the compiled quadrics) is projected onto the detector and
+    kept for every 16 x 16 pixel tile its footprint meets (the whole detector
+    when a corner is not in front of the source); every ray of a kept tile
+    tests the shape. FLOPs per test are the kernel's FP64 operations on the hit
+    path (a division or square root counting one): 12 for the ray direction in
+    the shape's frame, 17 (ellipsoid) or 18 (cylinder) for the quadric roots, 5
+    per clip plane and 3 for the additive accumulation.
+    """
+    from aprict_b200.cb import forbild
+
+    q = forbild.compile_shapes(shapes)
+    kind, nclip = q["kind"], q["n_clip"] & 0xFF
+    c = np.array([list(x) for x in q["c"]], np.float64)
+    bb = np.array([list(x) for x in q["bb_half"]], np.float64)
+    sgn = np.array([[(1 if k & 4 else -1), (1 if k & 2 else -1), (1 if k & 1 else -1)] for k in range(8)], np.float64)
+    X = c[:, None, :] + sgn[None] * bb[:, None, :]
+    flops_pair = np.where(kind == 1, 12 + 17, 12 + 18) + 5 * nclip + 3
+    flops_pair = np.where(kind == 0, 0, flops_pair)
+    specs = pg.to_proj_spec_array()
+    pairs = flops = 0
+    for sp in specs:
+        s = np.array([sp["source_pos"][k] for k in "xyz"], np.float64)
+        P = np.array([sp["det_pos"][k] for k in "xyz"], np.float64)  # noqa: N806
+        U = np.array([sp["det_u"][k] for k in "xyz"], np.float64)  # noqa: N806
+        V = np.array([sp["det_v"][k] for k in "xyz"], np.float64)  # noqa: N806
+        nu, nv = int(sp["nu"]), int(sp["nv"])
+        n = np.cross(U, V)
+        Ps = P - s  # noqa: N806
+        Dn = Ps @ n  # noqa: N806
+        Au = (U * Dn - n * (U @ Ps)) / (U @ U) + n * (nu - 1) / 2  # noqa: N806
+        Av = (V * Dn - n * (V @ Ps)) / (V @ V) + n * (nv - 1) / 2  # noqa: N806
+        r = X - s
+        den = r @ n
+        fu, fv = (r @ Au) / den, (r @ Av) / den
+        front = np.all(den * np.sign(Dn) > 0, axis=1)
+        tu = np.arange((nu + tile - 1) // tile)
+        tv = np.arange((nv + tile - 1) // tile)
+        u0, u1 = tu * tile - 0.5, np.minimum(nu, (tu + 1) * tile) - 0.5
+        v0, v1 = tv * tile - 0.5, np.minimum(nv, (tv + 1) * tile) - 0.5
+        ku = (fu.max(1)[:, None] >= u0[None] - 1e-6) & (fu.min(1)[:, None] <= u1[None] + 1e-6) | ~front[:, None]
+        kv = (fv.max(1)[:, None] >= v0[None] - 1e-6) & (fv.min(1)[:, None] <= v1[None] + 1e-6) | ~front[:, None]
+        rays_u = (np.minimum(nu, (tu + 1) * tile) - tu * tile)[None, :]
+        rays_v = (np.minimum(nv, (tv + 1) * tile) - tv * tile)[None, :]
+        tests = (ku * rays_u).sum(1) * (kv * rays_v).sum(1) * (kind != 0)
+        pairs += int(tests.sum())
+        flops += int((tests * flops_pair).sum())
+    return pairs, flops
 
 
 def run_component(args) -> dict:
@@ -906,10 +993,16 @@ def run_component(args) -> dict:
     cfg = fp.ConfigProject(overlap_addition=True)
     t_q = _timed(lambda: fp.project(cfg, vol, ps), args.steps)
     rays = w["views"] * w["det"] ** 2
+    pairs, flops = quadric_tests(pg, shapes)
+    fp64_peak = 148 * 64 * 2 * 1.965e9  # nominal FP64 FLOP/s (SMs x FP64 lanes x 2 x max SM clock)
     extra = {"components": {"project_ms": round(t_q, 3), "rays_per_s": round(rays / (t_q * 1e-3), 1),
                             "overflow_rays": int(ps.out_of_mem_count),
                             "output_GB": round(4 * rays / 1e9, 3),
-                            "output_write_GBps": round(4 * rays / (t_q * 1e-3) / 1e9, 1)}}
+                            "output_write_GBps": round(4 * rays / (t_q * 1e-3) / 1e9, 1),
+                            "ray_shape_tests": pairs,
+                            "fp64_flops_algorithmic": flops,
+                            "fp64_tflops_algorithmic": round(flops / (t_q * 1e-3) / 1e12, 3),
+                            "fp64_frac_of_nominal_peak": round(flops / (t_q * 1e-3) / fp64_peak, 4)}}
     return _line(args, "quadric projection rays/s", round(rays / (t_q * 1e-3), 1), "rays/s", t_q,
                  f"quadric: {len(shapes)} clipped quadrics in {2 * w['radius']:.0f} mm, {w['views']} views x {w['det']}^2 x {w['pix']} mm, additive", extra)
 
@@ -1112,6 +1205,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sirt256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch48", action="store_true", help="skip the batched uneven-scan section of the default line")
     ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

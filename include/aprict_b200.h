@@ -132,7 +132,8 @@ APRICT_API const char *aprict_b200_version(void);
  *   3 forward-projector warp patch height (lanes along v): 8, 16 or 32;
  *   4 forward-projector views per detector tile: 1, 2 or 4 (default 4);
  *   5 forward-projector views inside one warp's patch: 1, 2 or 4;
- *   6 one-scan forward projector with one sub-ray per pixel: 0 specialised path (default), 1 general path.
+ *   6 one-scan forward projector with one sub-ray per pixel: 0 specialised path (default), 1 general path;
+ *   7 one-scan backprojector on C-order volumes: 0 z-column layout when the volume is tall enough (default), 1 never.
  * Set by the autotuner (aprict_b200/autotune.py); results never depend on them. */
 APRICT_API int aprict_b200_set_tuning(int key, int value);
 APRICT_API int aprict_b200_get_tuning(int key);

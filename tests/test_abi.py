@@ -149,11 +149,11 @@ def test_volops_validation() -> None:
 
 def test_tuning_knobs_validate_and_round_trip() -> None:
     lib = _lib.lib()
-    saved = [lib.aprict_b200_get_tuning(k) for k in range(7)]
+    saved = [lib.aprict_b200_get_tuning(k) for k in range(8)]
     try:
         for key, good, bad in [(0, (0, 8, 16, 32), (7, 64, -1)), (1, (0, 2, 4, 8), (1, 3, 16)), (2, (0, 1, 16), (-1, 17)),
                                (3, (0, 8, 16, 32), (4, 64)), (4, (0, 1, 2, 4), (3, 8, -1)), (5, (0, 1, 2, 4), (3, 8)),
-                               (6, (0, 1), (2, -1))]:
+                               (6, (0, 1), (2, -1)), (7, (0, 1), (2, -1))]:
             for v in good:
                 assert lib.aprict_b200_set_tuning(key, v) == 0
                 assert lib.aprict_b200_get_tuning(key) == v
@@ -161,7 +161,7 @@ def test_tuning_knobs_validate_and_round_trip() -> None:
                 with pytest.raises(ValueError):
                     _lib.check(lib.aprict_b200_set_tuning(key, v), "set_tuning")
         with pytest.raises(ValueError):
-            _lib.check(lib.aprict_b200_set_tuning(7, 0), "set_tuning")
+            _lib.check(lib.aprict_b200_set_tuning(8, 0), "set_tuning")
         assert lib.aprict_b200_get_tuning(99) == 0
     finally:
         for k, v in enumerate(saved):
