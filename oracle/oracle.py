@@ -470,3 +470,95 @@ def ref_forbild_sample(shapes: np.ndarray, xs, ys, zs, *, ss_wid: float = 0.0, s
     lib.ref_forbild_sample(_p(sh), len(sh), _p(ax[0]), _p(ax[1]), _p(ax[2]), len(ax[0]), len(ax[1]), len(ax[2]),
                            ctypes.c_float(ss_wid), ss, _p(out), nthreads or nthreads_default())
     return out
+
+
+# ------------------------------------------------------- reference kernels on the GPU
+REF_GPU_SO = HERE / "_ref" / "libaprict_refgpu.so"
+
+
+def have_ref_gpu() -> bool:
+    """Whether the reference's GPU kernels were built (oracle/_ref/libaprict_refgpu.so)."""
+    return REF_GPU_SO.exists()
+
+
+class RefGpuVolume:
+    """A C-order float32 volume in a CUDA array behind a surface object, as the
+    reference's Texture holds it; the reference's own kernels read and write it.
+
+    ``src`` is a CUDA float32 tensor of shape (nx, ny, nz), C-contiguous."""
+
+    def __init__(self, src) -> None:  # noqa: ANN001
+        self._lib = _load(REF_GPU_SO)
+        self._lib.refgpu_vol_destroy.restype = None
+        nx, ny, nz = (int(s) for s in src.shape)
+        if not (src.is_cuda and src.is_contiguous() and str(src.dtype) == "torch.float32"):
+            msg = "the volume must be a C-contiguous float32 CUDA tensor"
+            raise ValueError(msg)
+        self.shape = (nx, ny, nz)
+        h = ctypes.c_void_p()
+        rc = self._lib.refgpu_vol_create(ctypes.c_void_p(src.data_ptr()), nx, ny, nz, ctypes.byref(h))
+        if rc != 0:
+            msg = f"refgpu_vol_create failed with CUDA error {rc}"
+            raise RuntimeError(msg)
+        self.handle = h
+
+    def read(self, dst, stream: int = 0) -> None:  # noqa: ANN001
+        _check_cuda(self._lib.refgpu_vol_read(self.handle, ctypes.c_void_p(dst.data_ptr()), ctypes.c_void_p(stream)),
+                    "refgpu_vol_read")
+
+    def write(self, src, stream: int = 0) -> None:  # noqa: ANN001
+        _check_cuda(self._lib.refgpu_vol_write(self.handle, ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(stream)),
+                    "refgpu_vol_write")
+
+    def close(self) -> None:
+        if self.handle:
+            self._lib.refgpu_vol_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001, S110
+            pass
+
+
+def _check_cuda(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = f"{what} failed with CUDA error {rc}"
+        raise RuntimeError(msg)
+
+
+def ref_gpu_project(vol: RefGpuVolume, specs_dev, n_views: int, nu: int, nv: int, out, *, voxwid: float,  # noqa: ANN001
+                    corner: np.ndarray, svf: float = 1.0, mba: float = 1.0, ssu: int = 1, ssv: int = 1,
+                    stream: int = 0) -> None:
+    """The reference's project_CB_texture_chunked<float,float>, launched as flatpanel.project
+    launches it; accumulates into ``out`` (a C-contiguous (n_views, nu, nv) float32 CUDA tensor)."""
+    lib = _load(REF_GPU_SO)
+    tp = np.asarray(corner, dtype=np.float32)
+    f = ctypes.c_float
+    _check_cuda(lib.refgpu_project(vol.handle, f(voxwid), _p(tp), ctypes.c_void_p(specs_dev), n_views, nu, nv,
+                                   ctypes.c_void_p(out.data_ptr()), f(svf), f(mba), ssu, ssv, ctypes.c_void_p(stream)),
+                "refgpu_project")
+
+
+def ref_gpu_backproject(vol: RefGpuVolume, specs: np.ndarray, projs, cfg_contents: np.ndarray, *,  # noqa: ANN001
+                        voxwid: float, corner: np.ndarray, mult: RefGpuVolume | None = None, stream: int = 0) -> None:
+    """The reference's backproject_CB_voltex<float,float>, launched as flatpanel.backproject
+    launches it (one launch per 10 views); adds into ``vol``. ``projs``: a C-contiguous
+    (n_views, nu, nv) float32 CUDA tensor; ``specs``: the host proj_spec records."""
+    lib = _load(REF_GPU_SO)
+    s = _specs(specs)
+    m, nu, nv = len(s), int(s["nu"][0]), int(s["nv"][0])
+    c = cfg_contents
+    if int(c["weighting_preset"]) != 0:
+        msg = "ref_gpu_backproject runs weighting preset 0 only"
+        raise ValueError(msg)
+    tp = np.asarray(corner, dtype=np.float32)
+    f = ctypes.c_float
+    _check_cuda(lib.refgpu_backproject(
+        vol.handle, None if mult is None else mult.handle, f(voxwid), _p(tp), _p(s), m, nu, nv,
+        ctypes.c_void_p(projs.data_ptr()), int(c["exact"]), int(c["backproject_all_1s"]), int(c["mask_to_cylinder"]),
+        f(float(c["mask_to_cyl_rad"])), f(float(c["soften_edge_proportion"])), int(c["Z_on_L_factor_power"]),
+        int(c["Z_on_val_factor_power"]), f(float(c["Z_on_val_factor_val"])), int(c["approx_mode_direct_raycast"]),
+        int(c["approx_mode_linear_interpolate"]), int(c["ssx"]), int(c["ssy"]), int(c["ssz"]),
+        ctypes.c_void_p(stream)), "refgpu_backproject")
