@@ -144,19 +144,20 @@ constexpr int batch_xb(int ord, bool exact) { return ord == 2 ? 2 : ab_bp::defau
 // a brick misses the detector: batches mix helical and circular scans, and
 // the helical ones leave most of a volume off each view's detector (48
 // uneven scans: 326.6 -> 265.3 ms per batched backprojection).
-template <int ORD, bool EXACT, bool RAYCAST, bool BILIN>
-__global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(batch_xb(ORD, EXACT), EXACT))
+template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB = batch_xb(ORD, EXACT)>
+__global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(XB, EXACT))
     k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
-    __shared__ ab_bp::BPSmem<EXACT, BILIN, batch_xb(ORD, EXACT)> sm;
+    __shared__ ab_bp::BPSmem<EXACT, BILIN, XB> sm;
     uint32_t unit;
     int s;
-    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, batch_xb(ORD, EXACT), true>(A.scans[s], unit, sm);
+    while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, XB, true>(A.scans[s], unit, sm);
     retire(A.g);
 }
 
 // Backprojection kernel variant code: ORD + 3 * mode (ORD from ab_bp::bp_ord),
 // mode 0 fast nearest, 1 fast bilinear, 2 raycast nearest, 3 raycast
-// bilinear, 4 exact; 15: fast nearest in the z-column layout (ORD 3).
+// bilinear, 4 exact; 15: fast nearest in the z-column layout (ORD 3) with 4
+// voxels per thread, 16: the same with 8 (every scan at least 256 voxels tall).
 int bp_variant(const aprict_backproject_config *c, const aprict_vol_desc *vd) {
     const int mode = c->exact ? 4
                               : (c->approx_mode_direct_raycast ? 2 : 0) + (c->approx_mode_linear_interpolate ? 1 : 0);
@@ -166,8 +167,12 @@ int bp_variant(const aprict_backproject_config *c, const aprict_vol_desc *vd) {
 // The batch backprojection kernel of a variant code.
 template <int V>
 auto bp_kernel() {
-    constexpr int ORD = V == 15 ? 3 : V % 3, mode = V == 15 ? 0 : V / 3;
-    return k_batch_backproject<ORD, mode == 4, mode == 2 || mode == 3, mode == 1 || mode == 3>;
+    if constexpr (V == 16) {
+        return k_batch_backproject<3, false, false, false, 8>;
+    } else {
+        constexpr int ORD = V == 15 ? 3 : V % 3, mode = V == 15 ? 0 : V / 3;
+        return k_batch_backproject<ORD, mode == 4, mode == 2 || mode == 3, mode == 1 || mode == 3>;
+    }
 }
 
 template <class F>
@@ -189,6 +194,7 @@ int with_bp_kernel(int variant, F &&f) {
         case 13: return f(bp_kernel<13>());
         case 14: return f(bp_kernel<14>());
         case 15: return f(bp_kernel<15>());
+        case 16: return f(bp_kernel<16>());
         default: return ab_fail(APRICT_ERR_INVALID_ARGUMENT, "corrupt batch plan (variant %d)", variant);
     }
 }
@@ -277,11 +283,14 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
     // qualifies (one kernel variant per plan; each scan then gets the layout
     // its one-scan call would take).
     bool zlanes = op == APRICT_BATCH_BACKPROJECT && n_scans > 0;
+    bool tall = true;  // every scan at least 256 voxels tall: 8 voxels per thread, as the one-scan call
     for (int i = 0; zlanes && i < n_scans; ++i) {
         const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
         const int xb = batch_xb(ab_bp::bp_ord(&scans[i].vol), cfg->exact != 0);
         zlanes = ab_bp::bp_zlanes_ok(&scans[i].vol, xb, cfg) && batch_xb(3, cfg->exact != 0) == xb;
+        tall = tall && scans[i].vol.nz >= 256u;
     }
+    const bool zl8 = zlanes && tall && ab_tuning_get(AB_TUNE_BP_XB) == 0;
     for (int i = 0; i < n_scans; ++i) {
         const aprict_scan &sc = scans[i];
         int rc;
@@ -302,10 +311,11 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
             int xb = 0, ord = -1;
             uint64_t u = 0;
             rc = ab_bp::make_bp_params(sc.specs_dev, &sc.projs, sc.projs_dev, &sc.vol, sc.vol_dev, sc.multiplier_dev,
-                                       cfg, sc.status_dev, bp[i], u, xb, batch_xb(ab_bp::bp_ord(&sc.vol), cfg->exact != 0),
+                                       cfg, sc.status_dev, bp[i], u, xb,
+                                       zl8 ? 8 : batch_xb(ab_bp::bp_ord(&sc.vol), cfg->exact != 0),
                                        zlanes ? &ord : nullptr);
             if (rc != APRICT_OK) return scan_error(rc, i);
-            const int v = ord == 3 ? 15 : bp_variant(cfg, &sc.vol);
+            const int v = ord == 3 ? (xb == 8 ? 16 : 15) : bp_variant(cfg, &sc.vol);
             if (variant >= 0 && v != variant)
                 return ab_fail(APRICT_ERR_INVALID_ARGUMENT,
                                "scan %d: every scan of a backprojection batch needs the same volume order, "

@@ -186,19 +186,6 @@ AB_HD bool ab_siddon_setup(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3]
     return true;
 }
 
-// Smallest of three crossings (never NaN: +inf for an axis the ray does not
-// cross). sm_100 has a three-input FP32 minimum: one ALU instruction in place
-// of two, in a loop whose ALU pipe is its busiest.
-AB_HD float ab_min3(float a, float b, float c) {
-#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-#else
-    return fminf(a, fminf(b, c));
-#endif
-}
-
 // One traversal step: tm is the next crossing; advances the state past it.
 // Branch-free: every lane of a warp runs the same instructions whichever axis
 // its ray crosses next. The three crossings are recomputed from their
@@ -290,7 +277,7 @@ AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3
     // value is loaded (in the grid: the step precedes the exit).
 #define AB_GATHER_STEP(part)                                   \
     do {                                                       \
-        const float tm_ = ab_min3(tx, ty, tz);                 \
+        const float tm_ = fminf(tx, fminf(ty, tz));            \
         part = fmaf(tm_ - t, mu, part);                        \
         t = tm_;                                               \
         AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm_); \

@@ -583,6 +583,102 @@ def simulate_data_cpu(pg, x_true: np.ndarray, w: dict, views: np.ndarray) -> np.
     return b
 
 
+def reference_gpu_sirt(w: dict, steps: int, warmup: int) -> dict:
+    """The reference's own GPU kernels on this GPU, in its SIRT iteration's launch pattern.
+
+    The reference's projector and backprojector kernel files, compiled unchanged
+    for sm_100a (oracle/_ref/libaprict_refgpu.so), launched as its flatpanel.project
+    / flatpanel.backproject launch them (32 x 20 threads per block over the
+    detector; 8 x 8 x 8 over the volume, one launch per 10 views), on volumes in
+    CUDA arrays behind surfaces. One step is the reference's SIRT iteration
+    (src/aprict/iterators/sirt_vram.py:130-152): copy b to the residual, project
+    the volume into it with multiply_before_adding = -1 and block, backproject
+    it into the volume with the preconditioner and block. The data are the same
+    phantom's projection by the reference's own projector with Poisson noise
+    (torch's generator, the workload's seed). Nothing of this library runs here.
+    """
+    import torch
+
+    from oracle import oracle
+
+    torch.cuda.set_device(0)
+    n, M = w["n"], w["views"]
+    pg, x_true = make_problem(w)
+    specs = pg.to_proj_spec_array()
+    specs_dev = torch.from_numpy(np.ascontiguousarray(specs).view(np.uint8).copy()).cuda()
+    corner = -np.float32(w["voxwid"]) * np.array((n, n, n), np.float32) / 2
+    det = w["det"]
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    vw = w["voxwid"]
+    # data: the reference's projection of the phantom, Poisson noise at the workload's photon count
+    xt = oracle.RefGpuVolume(torch.from_numpy(x_true).cuda().contiguous())
+    p = torch.zeros((M, det, det), dtype=torch.float32, device="cuda")
+    oracle.ref_gpu_project(xt, specs_dev.data_ptr(), M, det, det, p, voxwid=vw, corner=corner, stream=sp)
+    g = torch.Generator(device="cuda").manual_seed(w["seed"])
+    counts = torch.poisson(w["photons"] * torch.exp(-p.double()), generator=g).clamp_(min=1.0)
+    b = (-torch.log(counts / w["photons"])).clamp_(max=float(np.log(w["photons"]))).float().contiguous()
+    del counts, p
+    xt.close()
+    x = oracle.RefGpuVolume(torch.zeros((n, n, n), dtype=torch.float32, device="cuda"))
+    mult = oracle.RefGpuVolume(torch.full((n, n, n), 1e-3, dtype=torch.float32, device="cuda"))
+    r = torch.empty_like(b)
+    # the reference's config_CB_backproject fields for ConfigBackproject(fast_approx=True,
+    # cyl_mask_rad=n/2 voxwid, apply_summand_multiplier=True, soften_det_edges_proportion=0.05)
+    cfg = {"exact": 0, "backproject_all_1s": 0, "mask_to_cylinder": 1, "mask_to_cyl_rad": n / 2 * vw,
+           "soften_edge_proportion": 0.05, "Z_on_L_factor_power": 0, "Z_on_val_factor_power": 0,
+           "Z_on_val_factor_val": 1.0, "approx_mode_direct_raycast": 0, "approx_mode_linear_interpolate": 0,
+           "ssx": 1, "ssy": 1, "ssz": 1, "weighting_preset": 0}
+
+    def fp_only() -> None:
+        oracle.ref_gpu_project(x, specs_dev.data_ptr(), M, det, det, r, voxwid=vw, corner=corner, mba=-1.0, stream=sp)
+
+    def bp_only() -> None:
+        oracle.ref_gpu_backproject(x, specs, r, cfg, voxwid=vw, corner=corner, mult=mult, stream=sp)
+
+    def iterate() -> None:
+        r.copy_(b)
+        fp_only()
+        torch.cuda.synchronize()
+        bp_only()
+        torch.cuda.synchronize()
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn, k: int) -> float:
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    t_fp = timed(fp_only, 3)
+    t_bp = timed(bp_only, 3)
+    for _ in range(warmup):
+        iterate()
+    ms = timed(iterate, steps)
+    x.close()
+    mult.close()
+    rays, vv = M * det * det, n**3 * M
+    return {
+        "what": "the reference's own GPU kernels (its CB_project_texture_chunked.cu and CB_backproject.cu compiled "
+                "unchanged for sm_100a) in its SIRT iteration's launch pattern: copy, projection, 36 ten-view "
+                "backprojection launches, two host syncs per iteration",
+        "iter_per_s": round(1000.0 / ms, 4),
+        "ms_per_step": round(ms, 3),
+        "steps": steps,
+        "fp_ms": round(t_fp, 3),
+        "bp_ms": round(t_bp, 3),
+        "fwd_rays_per_s": round(rays / (t_fp * 1e-3), 1),
+        "back_voxel_updates_per_s": round(vv / (t_bp * 1e-3), 1),
+    }
+
+
 def run_reference(args) -> dict:
     rank, world, _ = _env_rank()
     if rank != 0:
@@ -607,6 +703,17 @@ def run_reference(args) -> dict:
     base = dict(vals[0])
     base["value"] = v
     sampled_ms = statistics.median(c["sampled_s"] for c in vals) * 1000.0
+    ref_gpu = None
+    if not args.no_reference_gpu:
+        try:
+            import torch
+
+            if torch.cuda.is_available() and oracle.have_ref_gpu():
+                ref_gpu = reference_gpu_sirt(w, steps=max(3, min(args.steps, 10)), warmup=2)
+            else:
+                ref_gpu = {"unavailable": "no GPU or the reference's GPU kernels are not built (oracle/Makefile ref)"}
+        except (RuntimeError, OSError) as exc:
+            ref_gpu = {"unavailable": f"{type(exc).__name__}: {exc}"[:200]}
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -639,6 +746,7 @@ def run_reference(args) -> dict:
         },
         "cpu_baseline": base,
         "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": ref_gpu,
     }
 
 
@@ -1206,6 +1314,8 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sirt256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch48", action="store_true", help="skip the batched uneven-scan section of the default line")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own kernels on the GPU")
     ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
