@@ -158,6 +158,7 @@ struct FPScan {
     int ssu, ssv;
     TileMap tm;
     uint32_t *status;
+    int one;  // 1, passed at run time (see AB_SIDDON_ADVANCE_I32)
 };
 
 // Rays of work unit b (block_tile order) of scan S; every thread of the CTA
@@ -174,7 +175,7 @@ __device__ __forceinline__ void fp_ray(const FPScan<Off> &S, int view, int iu, i
         const ab_d3 dst = ab_to_grid(S.g, ab_pixel_pos(sp, (double)iu, (double)iv) * (double)S.svf);
         VolLoad<Off> ld{S.vol, pol};
         float sum;
-        ab_siddon_gather<Off>(src, dst, S.g.n, S.g.stride, ld, sum, &bad);
+        ab_siddon_gather<Off>(src, dst, S.g.n, S.g.stride, ld, sum, &bad, S.one);
         tot = (sum * S.g.voxwid) * S.mba;
     } else {
         const aprict_proj_spec sp = S.specs[view];
@@ -191,7 +192,7 @@ __device__ __forceinline__ void fp_ray(const FPScan<Off> &S, int view, int iu, i
                 const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)S.svf);
                 VolLoad<Off> ld{S.vol, pol};
                 float sum;
-                ab_siddon_gather<Off>(src, dst, g.n, g.stride, ld, sum, &bad);
+                ab_siddon_gather<Off>(src, dst, g.n, g.stride, ld, sum, &bad, S.one);
                 accu += (sum * g.voxwid) * S.mba;
             }
             if (ssv > 1) accu /= (float)ssv;
@@ -254,6 +255,7 @@ inline FPScan<Off> make_fpscan(const aprict_proj_spec *specs, const aprict_proj_
     S.ssv = (int)cfg->ssv;
     S.tm = make_tiles(pd->nu, pd->nv, pd->n_views);
     S.status = status;
+    S.one = 1;
     units = (pd->n_views == 0 || pd->nu == 0 || pd->nv == 0) ? 0 : S.tm.units();
     return S;
 }
