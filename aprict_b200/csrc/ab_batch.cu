@@ -129,7 +129,8 @@ __device__ __forceinline__ void retire(Group *g) {
 }
 
 template <typename Off, bool SS1>
-__global__ void __launch_bounds__(ab_fp::kThreads, 4) k_batch_project(const __grid_constant__ BatchArgs<ab_fp::FPScan<Off>> A) {
+__global__ void __launch_bounds__(ab_fp::kThreads, ab_fp::fp_min_blocks(SS1))
+    k_batch_project(const __grid_constant__ BatchArgs<ab_fp::FPScan<Off>> A) {
     uint32_t unit;
     int s;
     while (next_unit(A, unit, s)) ab_fp::fp_tile<Off, SS1>(A.scans[s], unit);

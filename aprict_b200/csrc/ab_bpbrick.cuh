@@ -251,6 +251,7 @@ struct BPSmem {
     float box[6];             // the brick's box (low corner, high corner) relative to the volume centre
     int vcount;               // views of the chunk whose brick projection reaches the detector
     uint8_t off_det[kChunk];  // per view: the whole brick projects beyond one detector edge
+    uint8_t zinv[kChunk];     // per view: depth and u do not change along z (ORD 3 shares them)
     uint8_t vlist[kChunk];    // those views' indices in the chunk, in order
     uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];
     float qd[EXACT ? 1 : kWarps][EXACT ? 1 : 32 * XB];  // [lane * XB + k]
@@ -515,6 +516,10 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                                (a2 == 0 ? bt.nv.x : (a2 == 1 ? bt.nv.y : bt.nv.z)) * vws,
                                                (a2 == 0 ? bt.den.x : (a2 == 1 ? bt.den.y : bt.den.z)) * vws,
                                                (a2 == 0 ? bt.zl.x : (a2 == 1 ? bt.zl.y : bt.zl.z)) * vws);
+                        // exact zeros in the z coefficients, FP32 and FP64 alike (ORD 3 only)
+                        sm.zinv[t] = (uint8_t)(kZ && kNear && bt.den.z == 0.f && bt.nu.z == 0.f &&
+                                               (!needZ || bt.zl.z == 0.f) && svd[t].nu[2] == 0.0 &&
+                                               svd[t].den[2] == 0.0);
                     }
                     __syncthreads();
                     // The chunk's views whose projection of the brick reaches the
@@ -647,46 +652,45 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                             // the axis do not change along z (exact zeros in the per-view
                             // steps; warp-uniform): the thread's voxels share rD, fu, the
                             // weight and the u half of the pixel choice, computed once.
-                            const bool zinv = kZ && dD == 0.f && dNu == 0.f && (!needZ || dZ == 0.f);
+                            const bool zinv = kZ && kNear && !RAYCAST && sm.zinv[t];
                             if (zinv) {
+                                // Every lane of the warp has this x and y, so everything that
+                                // depends on u is warp-uniform: the u half of the pixel choice
+                                // (FP64 for a near tie), the u half of the edge taper and
+                                // whether the column lies on the detector are settled here
+                                // once; only v-side cases are deferred to the second pass.
                                 const float rD = rcp_fast(D0);
                                 const float fu = Nu0 * rD;
-                                float w = RAYCAST ? 1.f : rD * rD;
-                                if (needZ) {
-                                    w *= zpow(P, b, Zb);
-                                    if (RAYCAST && P.preset != 0)
-                                        w *= preset_weight(P.preset, P.val, X0 + P.c0[0], Y0 + P.c0[1], b.sxw, b.syw, Zb);
+                                float w = rD * rD;
+                                if (needZ) w *= zpow(P, b, Zb);
+                                float du;
+                                int iu = round_index(fu, -2.f, P.fnu1, du);
+                                if (fabsf(du) > b.tie_u) {
+                                    const VoxRef vr{((double)b2 + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                    ((double)i1 + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd, 0.0};
+                                    iu = refine_index(svd[t].nu, svd[t].den, vr, iu, du);
                                 }
-                                const float au = fabsf(fu - b.cu0);
-                                const bool inner_u = au <= b.tap_ru;
-                                const bool outside_u = kSkip && au > b.out_ru + (BILIN ? 0.5f : 0.f);
-                                const float tu = __fadd_rn(fu, kMagic);
-                                const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
-                                const bool fast_u = inner_u && fabsf(du) <= b.tie_u;
-                                const uint32_t offu = (uint32_t)__float_as_int(tu) * (uint32_t)P.su + P.koff;
+                                if ((unsigned)iu < P.nu) {  // else the column is off the detector: zeros
+                                    const float cu = fu - b.cu0;
+                                    if (P.sep > 0.f && fabsf(cu) > b.tap_ru)
+                                        w *= ab_edge_taper(cu, 0.f, b.inv_halfu, b.inv_halfv, P.inv_sep);
+                                    const uint32_t offu = (uint32_t)iu * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
 #pragma unroll
-                                for (int k = 0; k < kXB; ++k) {
-                                    const float fv = fmaf((float)k, dNv, Nv0) * rD;
-                                    const float av = fabsf(fv - b.cv0);
-                                    const bool outside = outside_u || (kSkip && av > b.out_rv + (BILIN ? 0.5f : 0.f));
-                                    float pv = 0.f;
-                                    bool fast;
-                                    if (BILIN) {
-                                        fast = inner_u && av <= b.tap_rv;
-                                        pv = fetch_bilinear(P, pvw, fu, fv);
-                                        pv = live[k] && fast ? pv : 0.f;
-                                        acc[k] = fmaf(pv, w, acc[k]);
-                                    } else {
+                                    for (int k = 0; k < kXB; ++k) {
+                                        const float fv = fmaf((float)k, dNv, Nv0) * rD;
+                                        const float av = fabsf(fv - b.cv0);
+                                        const bool outside = kSkip && av > b.out_rv;
                                         const float tv = __fadd_rn(fv, kMagic);
                                         const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
-                                        fast = fast_u && av <= b.tap_rv && fabsf(dv) <= b.tie_v;
+                                        const bool fast = av <= b.tap_rv && fabsf(dv) <= b.tie_v;
                                         const int off = (int)((uint32_t)__float_as_int(tv) * (uint32_t)P.sv + offu);
+                                        float pv = 0.f;
                                         if (live[k] && fast) pv = __ldg(pvw + off);
                                         acc[k] = fmaf(pvp[k], wp[k], acc[k]);
                                         pvp[k] = pv;
                                         wp[k] = w;
+                                        pending |= (live[k] && !fast && !outside) ? 1u << k : 0u;
                                     }
-                                    pending |= (live[k] && !fast && !outside) ? 1u << k : 0u;
                                 }
                             } else {
 #pragma unroll

@@ -24,6 +24,11 @@ namespace ab_fp {
 
 constexpr int kThreads = 256;
 
+// Resident CTAs per SM the projector kernels are compiled for: the
+// single-sub-ray ray path fits 48 registers without spilling, the general
+// (sub-ray) path keeps 64.
+constexpr int fp_min_blocks(bool ss1) { return ss1 ? 5 : 4; }
+
 struct TileMap {
     int tile_w, tile_u, tile_v;  // tile extents: views, pixels along u, pixels along v
     int warp_w, warp_u, warp_v;  // a warp's patch (product 32)

@@ -28,10 +28,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_project_siddon(const FPScan<Off
 // z: row band; the hardware issues blocks in that linear order), which saves
 // the per-thread division of a linear block index. With one sub-ray per pixel
 // the specialised ray path runs (no spills; 12.35 ms against 13.25 ms for the
-// general path on the 256^3 x 360-view fused residual, bit-identical results);
-// tuning knob 6 = 1 forces the general path.
+// general path on the 256^3 x 360-view fused residual, bit-identical results),
+// at 5 resident CTAs per SM (48 registers, no spills: 9.93 against 10.20 ms at
+// 4); tuning knob 6 = 1 forces the general path.
 template <typename Off, bool SS1>
-__global__ void __launch_bounds__(kThreads, 4) k_project_siddon_3d(const FPScan<Off> S) {
+__global__ void __launch_bounds__(kThreads, fp_min_blocks(SS1)) k_project_siddon_3d(const FPScan<Off> S) {
     int view, iu, iv;
     if (!tile_thread(S.tm, S.n_views, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, view, iu, iv) ||
         iu >= (int)S.nu || iv >= (int)S.nv)
