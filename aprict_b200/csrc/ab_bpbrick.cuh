@@ -673,7 +673,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                 if ((unsigned)iu < P.nu) {  // else the column is off the detector: zeros
                                     const float cu = fu - b.cu0;
                                     if (P.sep > 0.f && fabsf(cu) > b.tap_ru)
-                                        w *= ab_edge_taper(cu, 0.f, b.inv_halfu, b.inv_halfv, P.inv_sep);
+                                        w *= ab_edge_taper_half(fabsf(cu), b.inv_halfu, P.inv_sep);
                                     const uint32_t offu = (uint32_t)iu * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
 #pragma unroll
                                     for (int k = 0; k < kXB; ++k) {
@@ -747,13 +747,21 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                             }
                             }
                             if (__any_sync(0xffffffffu, pending != 0u)) {
+                                // each lane's deferred voxel-views go to consecutive queue
+                                // slots after those of the lower lanes (warp prefix sum)
+                                const int cnt = __popc(pending);
+                                int incl = cnt;
 #pragma unroll
-                                for (int k = 0; k < kXB; ++k) {
-                                    const bool p = (pending >> k) & 1u;
-                                    const unsigned m = __ballot_sync(0xffffffffu, p);
-                                    if (p) q[qn + __popc(m & ((1u << lane) - 1u))] = (uint16_t)((t << (5 + kKB)) | (k << 5) | lane);
-                                    qn += __popc(m);
+                                for (int o = 1; o < 32; o <<= 1) {
+                                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                                    if (lane >= o) incl += y;
                                 }
+                                int pos = qn + incl - cnt;
+                                for (unsigned pm = pending; pm != 0u; pm &= pm - 1u) {
+                                    const int k = __ffs(pm) - 1;
+                                    q[pos++] = (uint16_t)((t << (5 + kKB)) | (k << 5) | lane);
+                                }
+                                qn += __shfl_sync(0xffffffffu, incl, 31);
                                 __syncwarp();
                                 while (qn >= 32) flush(32, v0);
                             }

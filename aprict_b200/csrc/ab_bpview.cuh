@@ -179,17 +179,19 @@ AB_HD float ab_powint(float b, int e) {
     return a;
 }
 
-// Detector-edge cosine taper (CB_backproject.cu:694-713); cu, cv are
-// coordinates relative to the detector centre in pixels. Outside the edge
-// band the clamped argument is 1 and the factor is exactly 1, so the cosines
-// are only evaluated inside the band.
+// One axis's factor of the detector-edge cosine taper (CB_backproject.cu:694-713):
+// a = |c|, the distance in pixels from the detector centre along that axis.
+// Outside the edge band the clamped argument is 1 and the factor is exactly 1
+// (the cosine is only evaluated inside the band).
+AB_HD float ab_edge_taper_half(float a, float inv_half, float inv_sep) {
+    const float r = a * inv_half;
+    const float d = fmaxf(0.f, fminf(1.f, (1.f - r) * inv_sep));
+    if (d == 1.f) return 1.f;
+    return fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - d))) * 0.5f));
+}
+
+// The taper's weight at (cu, cv), pixels relative to the detector centre: the
+// product of the two axes' factors.
 AB_HD float ab_edge_taper(float cu, float cv, float inv_halfu, float inv_halfv, float inv_sep) {
-    float ud = fabsf(cu) * inv_halfu;
-    float vd = fabsf(cv) * inv_halfv;
-    ud = fmaxf(0.f, fminf(1.f, (1.f - ud) * inv_sep));
-    vd = fmaxf(0.f, fminf(1.f, (1.f - vd) * inv_sep));
-    if (ud == 1.f && vd == 1.f) return 1.f;
-    ud = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - ud))) * 0.5f));
-    vd = fmaxf(0.f, fminf(1.f, (1.f + cosf(3.1415926535898f * (1.f - vd))) * 0.5f));
-    return ud * vd;
+    return ab_edge_taper_half(fabsf(cu), inv_halfu, inv_sep) * ab_edge_taper_half(fabsf(cv), inv_halfv, inv_sep);
 }
