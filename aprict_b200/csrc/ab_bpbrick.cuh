@@ -675,6 +675,38 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                     if (P.sep > 0.f && fabsf(cu) > b.tap_ru)
                                         w *= ab_edge_taper_half(fabsf(cu), b.inv_halfu, P.inv_sep);
                                     const uint32_t offu = (uint32_t)iu * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
+                                    // Interior column: fv is monotone in k, so when the first and
+                                    // last voxel of every lane lie in the flat box, all of the
+                                    // warp's rows are on the detector with taper weight 1 and only
+                                    // a near-tie row choice remains. That pass has no predicates:
+                                    // it loads every voxel's FP32-rounded pixel (live or not; dead
+                                    // voxels are never written) and turns the tie test into an
+                                    // FMA-pipe value slow = 0 or 1 that zeroes the weight and sets
+                                    // the voxel's bit of the fix-up mask.
+                                    const float fvf = fmaf(0.f, dNv, Nv0) * rD;
+                                    const float fvl = fmaf((float)(kXB - 1), dNv, Nv0) * rD;
+                                    const bool inbox = fabsf(fvf - b.cv0) <= b.tap_rv && fabsf(fvl - b.cv0) <= b.tap_rv;
+                                    if (__all_sync(0xffffffffu, inbox) && b.tie_v >= 0.25f) {
+                                        // |dv| and tie_v lie in [0, 1/2] and tie_v >= 1/4: |dv| > tie_v
+                                        // means |dv| - tie_v >= 2^-25, so 2^40 (|dv| - tie_v)
+                                        // saturates to exactly 1, and to 0 otherwise
+                                        const float ntie = -b.tie_v * 0x1p40f;
+                                        float pendf = 0.f;
+#pragma unroll
+                                        for (int k = 0; k < kXB; ++k) {
+                                            const float fv = fmaf((float)k, dNv, Nv0) * rD;
+                                            const float tv = __fadd_rn(fv, kMagic);
+                                            const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
+                                            const float slow = __saturatef(fmaf(fabsf(dv), 0x1p40f, ntie));
+                                            const int off = (int)((uint32_t)__float_as_int(tv) * (uint32_t)P.sv + offu);
+                                            const float pv = __ldg(pvw + off);
+                                            acc[k] = fmaf(pvp[k], wp[k], acc[k]);
+                                            pvp[k] = pv;
+                                            wp[k] = fmaf(-slow, w, w);
+                                            pendf = fmaf(slow, (float)(1u << k), pendf);
+                                        }
+                                        pending = (unsigned)pendf;
+                                    } else {
 #pragma unroll
                                     for (int k = 0; k < kXB; ++k) {
                                         const float fv = fmaf((float)k, dNv, Nv0) * rD;
@@ -690,6 +722,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                         pvp[k] = pv;
                                         wp[k] = w;
                                         pending |= (live[k] && !fast && !outside) ? 1u << k : 0u;
+                                    }
                                     }
                                 }
                             } else {
