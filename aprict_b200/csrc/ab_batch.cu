@@ -288,7 +288,7 @@ extern "C" int aprict_b200_batch_plan(int op, const aprict_scan *scans, int n_sc
     for (int i = 0; zlanes && i < n_scans; ++i) {
         const aprict_backproject_config *cfg = static_cast<const aprict_backproject_config *>(configs) + i;
         const int xb = batch_xb(ab_bp::bp_ord(&scans[i].vol), cfg->exact != 0);
-        zlanes = ab_bp::bp_zlanes_ok(&scans[i].vol, xb, cfg) && batch_xb(3, cfg->exact != 0) == xb;
+        zlanes = ab_bp::bp_zlanes_ok(&scans[i].vol, &scans[i].projs, xb, cfg) && batch_xb(3, cfg->exact != 0) == xb;
         tall = tall && scans[i].vol.nz >= 256u;
     }
     const bool zl8 = zlanes && tall && ab_tuning_get(AB_TUNE_BP_XB) == 0;

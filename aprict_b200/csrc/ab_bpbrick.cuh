@@ -254,7 +254,11 @@ struct BPSmem {
     uint8_t zinv[kChunk];     // per view: depth and u do not change along z (ORD 3 shares them)
     uint8_t vlist[kChunk];    // those views' indices in the chunk, in order
     uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];
-    float qd[EXACT ? 1 : kWarps][EXACT ? 1 : 32 * XB];  // [lane * XB + k]
+    // Nearest mode, z-column layout: per warp, the warp-uniform part of 32
+    // consecutive views of the chunk (rD, weight, and the 64-bit byte address
+    // of the column's pixel 0 less 4 * 0x4B400000 * sv, split in two words; rD
+    // NaN when the warp's column misses the detector)
+    float4 zrec[kNear ? kWarps : 1][kNear ? 32 : 1];
     // Compensated per-voxel totals over the view chunks: sum and Kahan term,
     // [warp][lane * XB + k], each slot owned by one thread.
     float ksum[kWarps][32 * XB];
@@ -405,15 +409,10 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
     // finished by their own lane -- that would stall the other 31 lanes of
     // the warp -- but queued per warp as (view, voxel, lane) and finished 32
     // at a time, every lane on a different item, whenever 32 are queued and
-    // at the end of each view chunk. Their contributions are summed per
-    // (lane, voxel) in shared memory and added to the accumulators at the end.
+    // at the end of each view chunk. Their contributions are added to the
+    // voxels' totals in shared memory (ksum, shared-memory atomics).
     uint16_t *q = sm.q[EXACT ? 0 : warp];
-    float *qd = sm.qd[EXACT ? 0 : warp];
     int qn = 0;
-    if constexpr (!EXACT) {
-#pragma unroll
-        for (int k = 0; k < kXB; ++k) qd[lane * kXB + k] = 0.f;
-    }
 
     const float offx = 1.f / (float)P.ssx, offy = 1.f / (float)P.ssy, offz = 1.f / (float)P.ssz;
     const bool needZ = P.pL != 0 || P.pV != 0 || (RAYCAST && P.preset != 0);
@@ -481,7 +480,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                         }
                         float s = pv * w;
                         if (P.sep > 0.f && s != 0.f) s *= taper(bq, fu, fv, P.inv_sep);
-                        atomicAdd(&qd[L * kXB + k], s);
+                        atomicAdd(&ksum[L * kXB + k], s);
                     }
                     __syncwarp();
                     const int rem = qn - c;
@@ -543,6 +542,50 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                     if (!__any_sync(0xffffffffu, any_live)) continue;
                     const int n_list = kSkip ? sm.vcount : cn;
                     for (int j = 0; j < n_list; ++j) {
+                        if constexpr (kZ && kNear && !RAYCAST) {
+                            if ((j & 31) == 0) {
+                                // The warp's table for views j .. j + 31: every lane of
+                                // the warp has this x and y, so for a view whose depth and
+                                // u coordinate do not change along z (zinv) everything
+                                // that depends on u is warp-uniform -- the reciprocal
+                                // depth, the weight, the u half of the pixel choice (FP64
+                                // for a near tie), the u half of the edge taper and
+                                // whether the column lies on the detector. Lane L settles
+                                // view j + L once for the warp's 32 x XB voxels.
+                                const int jj = j + lane;
+                                const int tt = jj < n_list ? (kSkip ? (int)sm.vlist[jj] : jj) : 0;
+                                if (jj < n_list && sm.zinv[tt]) {
+                                    const ab_bpview bq = sv[tt];
+                                    const float rDq = rcp_fast(dot4(bq.den, X0, Y0, Z0));
+                                    const float fu = dot4(bq.nu, X0, Y0, Z0) * rDq;
+                                    float w = rDq * rDq;
+                                    if (needZ) w *= zpow(P, bq, dot4(bq.zl, X0, Y0, Z0));
+                                    float du;
+                                    int iu = round_index(fu, -2.f, P.fnu1, du);
+                                    if (fabsf(du) > bq.tie_u) {
+                                        const VoxRef vr{((double)b2 + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                        ((double)i1 + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                        0.0};
+                                        iu = refine_index(svd[tt].nu, svd[tt].den, vr, iu, du);
+                                    }
+                                    float4 rec = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+                                    if ((unsigned)iu < P.nu) {
+                                        const float cu = fu - bq.cu0;
+                                        if (P.sep > 0.f && fabsf(cu) > bq.tap_ru)
+                                            w *= ab_edge_taper_half(fabsf(cu), bq.inv_halfu, P.inv_sep);
+                                        // + 4 sv bits(tv) is then the byte address of row round(fv)
+                                        const uint64_t col =
+                                            (uint64_t)(uintptr_t)(P.projs + (int64_t)(v0 + tt) * P.stride_view +
+                                                                  (int64_t)iu * P.su) -
+                                            4ull * 0x4B400000ull * (uint64_t)(uint32_t)P.sv;
+                                        rec = make_float4(rDq, w, __uint_as_float((uint32_t)col),
+                                                          __uint_as_float((uint32_t)(col >> 32)));
+                                    }
+                                    sm.zrec[warp][lane] = rec;
+                                }
+                                __syncwarp();
+                            }
+                        }
                         const int t = kSkip ? (int)sm.vlist[j] : j;
                         const int view = (int)v0 + t;
                         const ab_bpview b = sv[t];
@@ -654,27 +697,13 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                             // weight and the u half of the pixel choice, computed once.
                             const bool zinv = kZ && kNear && !RAYCAST && sm.zinv[t];
                             if (zinv) {
-                                // Every lane of the warp has this x and y, so everything that
-                                // depends on u is warp-uniform: the u half of the pixel choice
-                                // (FP64 for a near tie), the u half of the edge taper and
-                                // whether the column lies on the detector are settled here
-                                // once; only v-side cases are deferred to the second pass.
-                                const float rD = rcp_fast(D0);
-                                const float fu = Nu0 * rD;
-                                float w = rD * rD;
-                                if (needZ) w *= zpow(P, b, Zb);
-                                float du;
-                                int iu = round_index(fu, -2.f, P.fnu1, du);
-                                if (fabsf(du) > b.tie_u) {
-                                    const VoxRef vr{((double)b2 + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
-                                                    ((double)i1 + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd, 0.0};
-                                    iu = refine_index(svd[t].nu, svd[t].den, vr, iu, du);
-                                }
-                                if ((unsigned)iu < P.nu) {  // else the column is off the detector: zeros
-                                    const float cu = fu - b.cu0;
-                                    if (P.sep > 0.f && fabsf(cu) > b.tap_ru)
-                                        w *= ab_edge_taper_half(fabsf(cu), b.inv_halfu, P.inv_sep);
-                                    const uint32_t offu = (uint32_t)iu * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
+                                // the warp-uniform part from the warp's table (filled above)
+                                const float4 rec = sm.zrec[warp][j & 31];
+                                const float rD = rec.x;
+                                if (rD == rD) {  // else the column is off the detector: zeros
+                                    const float w = rec.y;
+                                    const uint64_t col = ((uint64_t)__float_as_uint(rec.w) << 32) | __float_as_uint(rec.z);
+                                    const uint32_t sv4 = 4u * (uint32_t)P.sv;
                                     // Interior column: fv is monotone in k, so when the first and
                                     // last voxel of every lane lie in the flat box, all of the
                                     // warp's rows are on the detector with taper weight 1 and only
@@ -698,8 +727,8 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                             const float tv = __fadd_rn(fv, kMagic);
                                             const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
                                             const float slow = __saturatef(fmaf(fabsf(dv), 0x1p40f, ntie));
-                                            const int off = (int)((uint32_t)__float_as_int(tv) * (uint32_t)P.sv + offu);
-                                            const float pv = __ldg(pvw + off);
+                                            const float pv = __ldg(reinterpret_cast<const float *>(
+                                                col + (uint64_t)(uint32_t)__float_as_int(tv) * sv4));
                                             acc[k] = fmaf(pvp[k], wp[k], acc[k]);
                                             pvp[k] = pv;
                                             wp[k] = fmaf(-slow, w, w);
@@ -715,9 +744,10 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
                                         const float tv = __fadd_rn(fv, kMagic);
                                         const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
                                         const bool fast = av <= b.tap_rv && fabsf(dv) <= b.tie_v;
-                                        const int off = (int)((uint32_t)__float_as_int(tv) * (uint32_t)P.sv + offu);
                                         float pv = 0.f;
-                                        if (live[k] && fast) pv = __ldg(pvw + off);
+                                        if (live[k] && fast)
+                                            pv = __ldg(reinterpret_cast<const float *>(
+                                                col + (uint64_t)(uint32_t)__float_as_int(tv) * sv4));
                                         acc[k] = fmaf(pvp[k], wp[k], acc[k]);
                                         pvp[k] = pv;
                                         wp[k] = w;
@@ -831,11 +861,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSm
 #pragma unroll
         for (int k = 0; k < kXB; ++k) acc[k] = fmaf(pvp[k], wp[k], acc[k]);
     }
-    if constexpr (!EXACT) {  // the deferred contributions (all sub-samples)
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < kXB; ++k) acc[k] += qd[lane * kXB + k];
-    }
+    __syncwarp();
 #pragma unroll
     for (int k = 0; k < kXB; ++k) acc[k] = ksum[lane * kXB + k] + (acc[k] - kcomp[lane * kXB + k]);
 
@@ -859,12 +885,15 @@ inline int bp_ord(const aprict_vol_desc *vd) { return vd->order == 0 ? (vd->nz =
 
 // Host: whether ORD 3 (lanes and a thread's voxels along z) applies: the
 // fast nearest mode on a C-order volume tall enough to fill the 32 XB voxels
-// of a thread column, unless tuning knob 7 is 1. Measured on a 256^3 volume
-// with 360 views: nearest 9.82 -> 8.68 ms; bilinear (27.4 vs 28.1 ms) and
-// exact (114.6 vs 115.2 ms) keep ORD 0.
-inline bool bp_zlanes_ok(const aprict_vol_desc *vd, int xb, const aprict_backproject_config *cfg) {
+// of a thread column, unless tuning knob 7 is 1, with a v stride below 2^30
+// elements (the gathers form their byte address as a 32 x 32-bit product).
+// Measured on a 256^3 volume with 360 views: nearest 9.82 -> 8.68 ms; bilinear
+// (27.4 vs 28.1 ms) and exact (114.6 vs 115.2 ms) keep ORD 0.
+inline bool bp_zlanes_ok(const aprict_vol_desc *vd, const aprict_proj_desc *pd, int xb,
+                         const aprict_backproject_config *cfg) {
     return bp_ord(vd) == 0 && ab_tuning_get(AB_TUNE_BP_ZLANES) != 1 && vd->nz >= 32u * (uint32_t)xb &&
-           !cfg->exact && !cfg->approx_mode_direct_raycast && !cfg->approx_mode_linear_interpolate;
+           pd->stride_v < (int64_t)1 << 30 && !cfg->exact && !cfg->approx_mode_direct_raycast &&
+           !cfg->approx_mode_linear_interpolate;
 }
 
 // Host: validate one backprojection call and fill its parameters; units is
@@ -954,7 +983,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     const int knob = ab_tuning_get(AB_TUNE_BP_XB);
     const bool forced = force_xb == 2 || force_xb == 4 || force_xb == 8;
     xb = forced ? force_xb : (knob == 2 || knob == 4 || knob == 8 ? knob : default_xb(cfg->exact != 0));
-    const int ord = ord_out && bp_zlanes_ok(vd, xb, cfg) ? 3 : bp_ord(vd);
+    const int ord = ord_out && bp_zlanes_ok(vd, pd, xb, cfg) ? 3 : bp_ord(vd);
     if (ord_out) *ord_out = ord;
     // z columns of 8 voxels per thread where the volume is tall enough (the
     // per-view work of a thread is shared by twice as many voxels: sirt256
