@@ -1317,10 +1317,23 @@ def main() -> None:
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference's own kernels on the GPU")
     ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
+    ap.add_argument("--tuning", default="",
+                    help="--mode kernels only: tile-shape knobs for A/B captures, e.g. fp_tile_v=16,fp_warp_v=16 "
+                         "(the names of aprict_b200.autotune)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if args.tuning and args.mode != "kernels":
+        ap.error("--tuning applies to --mode kernels only")
     if args.mode == "kernels":
+        if args.tuning:
+            from aprict_b200 import autotune
+
+            knobs = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
+            known = {"fp_tile_v", "fp_warp_v", "fp_views", "fp_warp_views", "bp_xb", "bp_wave", "fp_ss1", "bp_zlanes"}
+            if set(knobs) - known:
+                ap.error(f"--tuning: unknown knobs {sorted(set(knobs) - known)}")
+            autotune.apply(knobs)
         out = profile_kernels(args)
     else:
         if args.impl == "reference":
