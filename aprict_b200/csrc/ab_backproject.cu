@@ -10,7 +10,7 @@ using namespace ab_bp;
 
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB>
 __global__ void __launch_bounds__(kThreads, bp_min_blocks(XB, EXACT)) k_backproject(const BPParams P) {
-    __shared__ BPSmem<EXACT, BILIN, XB> sm;
+    __shared__ BPSmem<EXACT, BILIN, XB, bp_ztable(ORD, EXACT, RAYCAST, BILIN)> sm;
     bp_brick<ORD, EXACT, RAYCAST, BILIN, XB>(P, blockIdx.x, sm);
 }
 

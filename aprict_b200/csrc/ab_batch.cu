@@ -148,7 +148,7 @@ constexpr int batch_xb(int ord, bool exact) { return ord == 2 ? 2 : ab_bp::defau
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB = batch_xb(ORD, EXACT)>
 __global__ void __launch_bounds__(ab_bp::kThreads, ab_bp::bp_min_blocks(XB, EXACT))
     k_batch_backproject(const __grid_constant__ BatchArgs<ab_bp::BPParams> A) {
-    __shared__ ab_bp::BPSmem<EXACT, BILIN, XB> sm;
+    __shared__ ab_bp::BPSmem<EXACT, BILIN, XB, ab_bp::bp_ztable(ORD, EXACT, RAYCAST, BILIN)> sm;
     uint32_t unit;
     int s;
     while (next_unit(A, unit, s)) ab_bp::bp_brick<ORD, EXACT, RAYCAST, BILIN, XB, true>(A.scans[s], unit, sm);

@@ -239,7 +239,11 @@ constexpr int bp_min_blocks(int xb, bool exact) { return exact ? kExactBlocks : 
 // per-voxel footprint loop gains nothing from sharing a view's coefficients).
 constexpr int default_xb(bool exact) { return exact ? 2 : 4; }
 
-template <bool EXACT, bool BILIN, int XB>
+// Whether a kernel variant keeps the per-warp view table (the z-column
+// layout's fast nearest mode).
+constexpr bool bp_ztable(int ord, bool exact, bool raycast, bool bilin) { return ord == 3 && !exact && !raycast && !bilin; }
+
+template <bool EXACT, bool BILIN, int XB, bool ZT = false>
 struct BPSmem {
     static constexpr bool kNear = !EXACT && !BILIN;
     static constexpr int kQCap = 32 + 32 * XB;  // a flush leaves < 32; one view adds <= 32 * XB
@@ -258,7 +262,7 @@ struct BPSmem {
     // consecutive views of the chunk (rD, weight, and the 64-bit byte address
     // of the column's pixel 0 less 4 * 0x4B400000 * sv, split in two words; rD
     // NaN when the warp's column misses the detector)
-    float4 zrec[kNear ? kWarps : 1][kNear ? 32 : 1];
+    float4 zrec[ZT ? kWarps : 1][ZT ? 32 : 1];
     // Compensated per-voxel totals over the view chunks: sum and Kahan term,
     // [warp][lane * XB + k], each slot owned by one thread.
     float ksum[kWarps][32 * XB];
@@ -269,7 +273,8 @@ struct BPSmem {
 // all views. Every thread of the CTA calls it with the same brick; it contains
 // __syncthreads and returns uniformly.
 template <int ORD, bool EXACT, bool RAYCAST, bool BILIN, int XB, bool SKIP = RAYCAST>
-__device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick, BPSmem<EXACT, BILIN, XB> &sm) {
+__device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
+                                         BPSmem<EXACT, BILIN, XB, bp_ztable(ORD, EXACT, RAYCAST, BILIN)> &sm) {
     static_assert(XB == 2 || XB == 4 || XB == 8, "XB is 2, 4 or 8");
     constexpr int kXB = XB, kKB = q_kbits<XB>();
     constexpr int kChunk = chunk_views<XB>();
