@@ -67,6 +67,7 @@ struct BPParams {
     float inv_val;  // 1 / val
     int preset;     // direct-raycast weighting preset 0-6
     int ssx, ssy, ssz;
+    int wide;  // su, sv < 2^30: byte addresses as two 32 x 32 -> 64-bit multiply-adds
     uint32_t *status;
 };
 
@@ -170,6 +171,33 @@ __device__ __forceinline__ bool brick_off_detector(const ab_bpview &b, const flo
     return front && (umin > eu || umax < -eu || vmin > ev || vmax < -ev);
 }
 
+// True when every point of the box [lo, hi] (relative to the volume centre)
+// projects, in the FP32 evaluation of the fast modes, into the flat box of the
+// detector-edge taper (inside the detector, taper weight exactly 1). The exact
+// projection of the box lies within the hull of its corners' projections
+// when all of them lie in front of the source; the FP32 coordinates of the
+// corners and of any voxel each carry at most the view's error bound, which
+// is below (1/2 - tie) / 1.5, so two bounds plus 1e-3 pixel are kept free.
+__device__ __forceinline__ bool brick_in_flat_box(const ab_bpview &b, const float lo[3], const float hi[3]) {
+    float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+    bool front = true;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float x = (c & 4) ? hi[0] : lo[0], y = (c & 2) ? hi[1] : lo[1], z = (c & 1) ? hi[2] : lo[2];
+        const float D = dot4(b.den, x, y, z);
+        front = front && D > 0.f;
+        const float rD = rcp_fast(D);
+        const float fu = dot4(b.nu, x, y, z) * rD - b.cu0, fv = dot4(b.nv, x, y, z) * rD - b.cv0;
+        umin = fminf(umin, fu);
+        umax = fmaxf(umax, fu);
+        vmin = fminf(vmin, fv);
+        vmax = fmaxf(vmax, fv);
+    }
+    const float mu = (0.5f - b.tie_u) * (4.f / 3.f) + 1e-3f, mv = (0.5f - b.tie_v) * (4.f / 3.f) + 1e-3f;
+    return front && umin - mu >= -b.tap_ru && umax + mu <= b.tap_ru && vmin - mv >= -b.tap_rv &&
+           vmax + mv <= b.tap_rv;
+}
+
 // x^e for a small integer e with one approximate reciprocal for e < 0
 // (relative error ~1e-6; the reference divides e times, CB_backproject.cu:21-35).
 __device__ __forceinline__ float powi_fast(float x, int e) {
@@ -253,6 +281,8 @@ struct BPSmem {
     ab_bpview_d svd[kNear ? kChunk : 1];
     ab_bpview_exact sx[EXACT ? kChunk : 1];
     float box[6];             // the brick's box (low corner, high corner) relative to the volume centre
+    float boxa[6];            // the box of every thread's voxels (not clipped to the volume)
+    uint8_t inner[kChunk];    // per view: every voxel of the CTA projects into the flat box
     int vcount;               // views of the chunk whose brick projection reaches the detector
     uint8_t off_det[kChunk];  // per view: the whole brick projects beyond one detector edge
     uint8_t zinv[kChunk];     // per view: depth and u do not change along z (ORD 3 shares them)
@@ -359,31 +389,39 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
     // their slice, so they skip nothing and keep the plain loop (the skip's
     // per-view work measured 15 % on 64 fan-beam slices).
     constexpr bool kSkip = SKIP && !EXACT && ORD != 2;
+    // Interior bricks (fast nearest mode, not direct-raycast): in a view that
+    // projects the whole brick into the detector's flat box, only near-tie
+    // pixel choices can need the second pass, and the voxels take a
+    // predicate-free pass (see the view loop).
+    constexpr bool kInt = !EXACT && !BILIN && !RAYCAST;
     // The brick's box relative to the volume centre (voxel faces, clipped to
     // the volume): every sub-sample of its voxels lies inside. Kept in shared
     // memory for the per-view off-detector test (ordered by the chunk loop's
     // first barrier).
-    if (kSkip && threadIdx.x == 0) {
-        int lo[3], hi[3];
+    if ((kSkip || kInt) && threadIdx.x == 0) {
+        int lo[3], hi[3], ha[3];
         if constexpr (kZ) {
             lo[0] = b2;
             hi[0] = b2 + 1;
             lo[1] = b1 * 8;
-            hi[1] = min(b1 * 8 + 8, P.n[1]);
+            ha[1] = b1 * 8 + 8;
             lo[2] = b0 * 32 * kXB;
-            hi[2] = min(lo[2] + 32 * kXB, P.n[2]);
+            ha[2] = lo[2] + 32 * kXB;
+            ha[0] = hi[0];
         } else {
             lo[a0] = b0 * 32;
-            hi[a0] = min(b0 * 32 + 32, P.n[a0]);
+            ha[a0] = b0 * 32 + 32;
             lo[a1] = ORD == 2 ? 0 : b1 * 8;
-            hi[a1] = ORD == 2 ? 1 : min(b1 * 8 + 8, P.n[a1]);
+            ha[a1] = ORD == 2 ? 1 : b1 * 8 + 8;
             lo[a2] = ORD == 2 ? b1 * 8 * kXB : i2b;
-            hi[a2] = min(lo[a2] + (ORD == 2 ? 8 * kXB : kXB), P.n[a2]);
+            ha[a2] = lo[a2] + (ORD == 2 ? 8 * kXB : kXB);
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            sm.box[a] = ((float)lo[a] - 0.5f * (float)P.n[a]) * vw;
+            if (!(kZ && a == 0)) hi[a] = min(ha[a], P.n[a]);
+            sm.box[a] = sm.boxa[a] = ((float)lo[a] - 0.5f * (float)P.n[a]) * vw;
             sm.box[3 + a] = ((float)hi[a] - 0.5f * (float)P.n[a]) * vw;
+            sm.boxa[3 + a] = ((float)ha[a] - 0.5f * (float)P.n[a]) * vw;
         }
     }
 
@@ -515,6 +553,9 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                         if (EXACT) ab_derive_bpview_exact(sp, c0d, sx[t]);
                         const ab_bpview &bt = sv[t];
                         if (kSkip) sm.off_det[t] = brick_off_detector(bt, sm.box, sm.box + 3, BILIN ? 0.5f : 0.f);
+                        if (kInt)
+                            sm.inner[t] = (uint8_t)(P.wide && bt.tie_u >= 0.25f && bt.tie_v >= 0.25f &&
+                                                    brick_in_flat_box(bt, sm.boxa, sm.boxa + 3));
                         const float vws = vw * (float)kStride;
                         sm.sd[t] = make_float4((a2 == 0 ? bt.nu.x : (a2 == 1 ? bt.nu.y : bt.nu.z)) * vws,
                                                (a2 == 0 ? bt.nv.x : (a2 == 1 ? bt.nv.y : bt.nv.z)) * vws,
@@ -760,6 +801,44 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                     }
                                     }
                                 }
+                            } else if (kInt && sm.inner[t]) {
+                                // Interior brick: every voxel's pixel is on the detector with
+                                // taper weight 1, so the pass has no predicates; it loads every
+                                // voxel's FP32-rounded pixel (dead voxels are never written) and
+                                // turns the u and v near-tie tests into an FMA-pipe value slow =
+                                // 0 or 1 (as in the z-column interior columns) that zeroes the
+                                // weight and sets the voxel's bit of the fix-up mask. Byte
+                                // addresses: two 32 x 32 -> 64-bit multiply-adds of the rounded
+                                // indices' bit patterns onto the view's base less the magic bias.
+                                const float ntu = -b.tie_u * 0x1p40f, ntv = -b.tie_v * 0x1p40f;
+                                const uint64_t vb = (uint64_t)(uintptr_t)pvw -
+                                                    4ull * 0x4B400000ull *
+                                                        ((uint64_t)(uint32_t)P.su + (uint64_t)(uint32_t)P.sv);
+                                const uint32_t su4 = 4u * (uint32_t)P.su, sv4 = 4u * (uint32_t)P.sv;
+                                float pendf = 0.f;
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    const float kf = (float)k;
+                                    const float D = fmaf(kf, dD, D0);
+                                    const float rD = rcp_fast(D);
+                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                    const float fv = fmaf(kf, dNv, Nv0) * rD;
+                                    float w = rD * rD;
+                                    if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
+                                    const float tu = __fadd_rn(fu, kMagic), tv = __fadd_rn(fv, kMagic);
+                                    const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
+                                    const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
+                                    const float slow = __saturatef(__saturatef(fmaf(fabsf(du), 0x1p40f, ntu)) +
+                                                                   __saturatef(fmaf(fabsf(dv), 0x1p40f, ntv)));
+                                    const float pv = __ldg(reinterpret_cast<const float *>(
+                                        vb + (uint64_t)(uint32_t)__float_as_int(tu) * su4 +
+                                        (uint64_t)(uint32_t)__float_as_int(tv) * sv4));
+                                    acc[k] = fmaf(pvp[k], wp[k], acc[k]);
+                                    pvp[k] = pv;
+                                    wp[k] = fmaf(-slow, w, w);
+                                    pendf = fmaf(slow, (float)(1u << k), pendf);
+                                }
+                                pending = (unsigned)pendf;
                             } else {
 #pragma unroll
                             for (int k = 0; k < kXB; ++k) {
@@ -945,6 +1024,7 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     P.su = (int)pd->stride_u;
     P.sv = (int)pd->stride_v;
     P.koff = 0u - 0x4B400000u * (uint32_t)P.su - 0x4B400000u * (uint32_t)P.sv;
+    P.wide = pd->stride_u < ((int64_t)1 << 30) && pd->stride_v < ((int64_t)1 << 30);
     P.fnu1 = (float)pd->nu + 1.f;
     P.fnv1 = (float)pd->nv + 1.f;
     P.projs = projs_dev;
