@@ -389,11 +389,11 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
     // their slice, so they skip nothing and keep the plain loop (the skip's
     // per-view work measured 15 % on 64 fan-beam slices).
     constexpr bool kSkip = SKIP && !EXACT && ORD != 2;
-    // Interior bricks (fast nearest mode, not direct-raycast): in a view that
-    // projects the whole brick into the detector's flat box, only near-tie
-    // pixel choices can need the second pass, and the voxels take a
+    // Interior bricks (nearest-pixel fast and direct-raycast modes): in a view
+    // that projects the whole brick into the detector's flat box, only
+    // near-tie pixel choices can need the second pass, and the voxels take a
     // predicate-free pass (see the view loop).
-    constexpr bool kInt = !EXACT && !BILIN && !RAYCAST;
+    constexpr bool kInt = !EXACT && !BILIN;
     // The brick's box relative to the volume centre (voxel faces, clipped to
     // the volume): every sub-sample of its voxels lies inside. Kept in shared
     // memory for the per-view off-detector test (ordered by the chunk loop's
@@ -823,8 +823,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                     const float rD = rcp_fast(D);
                                     const float fu = fmaf(kf, dNu, Nu0) * rD;
                                     const float fv = fmaf(kf, dNv, Nv0) * rD;
-                                    float w = rD * rD;
-                                    if (needZ) w *= zpow(P, b, fmaf(kf, dZ, Zb));
+                                    float w = RAYCAST ? 1.f : rD * rD;
+                                    if (needZ) {
+                                        const float Zk = fmaf(kf, dZ, Zb);
+                                        w *= zpow(P, b, Zk);
+                                        if (RAYCAST && P.preset != 0)
+                                            w *= preset_weight(P.preset, P.val, X0 + (a2 == 0 ? kf * vw : 0.f) + P.c0[0],
+                                                               Y0 + P.c0[1], b.sxw, b.syw, Zk);
+                                    }
                                     const float tu = __fadd_rn(fu, kMagic), tv = __fadd_rn(fv, kMagic);
                                     const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
                                     const float dv = __fsub_rn(fv, __fsub_rn(tv, kMagic));
