@@ -139,6 +139,16 @@ __device__ __forceinline__ float rcp_fast(float x) {
     return r;
 }
 
+// sqrt with one MUFU op (relative error ~2^-22), for the exact mode's chord
+// lengths. The reference builds its kernels with -use_fast_math
+// (src/aprict/cuda/header_injection.py:54-59), where sqrtf is this
+// approximation as well.
+__device__ __forceinline__ float sqrt_fast(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ float taper(const ab_bpview &b, float fu, float fv, float inv_sep) {
     if (fabsf(fu - b.cu0) <= b.tap_ru && fabsf(fv - b.cv0) <= b.tap_rv) return 1.f;
     return ab_edge_taper(fu - b.cu0, fv - b.cv0, b.inv_halfu, b.inv_halfv, inv_sep);
@@ -562,9 +572,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                                (a2 == 0 ? bt.den.x : (a2 == 1 ? bt.den.y : bt.den.z)) * vws,
                                                (a2 == 0 ? bt.zl.x : (a2 == 1 ? bt.zl.y : bt.zl.z)) * vws);
                         // exact zeros in the z coefficients, FP32 and FP64 alike (ORD 3 only)
-                        sm.zinv[t] = (uint8_t)(kZ && kNear && bt.den.z == 0.f && bt.nu.z == 0.f &&
-                                               (!needZ || bt.zl.z == 0.f) && svd[t].nu[2] == 0.0 &&
-                                               svd[t].den[2] == 0.0);
+                        if constexpr (EXACT)  // and the detector's v axis has no x-y component
+                            sm.zinv[t] = (uint8_t)(kZ && bt.den.z == 0.f && bt.nu.z == 0.f &&
+                                                   (!needZ || bt.zl.z == 0.f) && sx[t].v.x == 0.f &&
+                                                   sx[t].v.y == 0.f);
+                        else
+                            sm.zinv[t] = (uint8_t)(kZ && kNear && bt.den.z == 0.f && bt.nu.z == 0.f &&
+                                                   (!needZ || bt.zl.z == 0.f) && svd[t].nu[2] == 0.0 &&
+                                                   svd[t].den[2] == 0.0);
                     }
                     __syncthreads();
                     // The chunk's views whose projection of the brick reaches the
@@ -646,6 +661,111 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                             dZ = steps.w;
                         }
                         if constexpr (EXACT) {
+                            if (kZ && sm.zinv[t]) {
+                                // Upright detector in the z-column layout: the thread's voxels
+                                // share x and y, so the depth and u of the column's four
+                                // vertical edges, the footprint's pixel columns and, per pixel
+                                // column, the x-y slab of its rays (whose x and y do not depend
+                                // on the row) are computed once per thread and view; per voxel
+                                // only the v extent and, per pixel, the z slab remain. The
+                                // arithmetic per quantity is the per-voxel path's.
+                                const ab_bpview_exact e = sx[t];
+                                const float h = 0.5f * vw;
+                                const float hd0 = b.den.x * h, hd1 = b.den.y * h;
+                                const float hu0 = b.nu.x * h, hu1 = b.nu.y * h;
+                                const float hv0 = b.nv.x * h, hv1 = b.nv.y * h, hv2 = b.nv.z * h;
+                                float rr[4], bv[4];
+                                float umin = 3.0e38f, umax = -3.0e38f;
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) {
+                                    const float sx_ = (c & 2) ? 1.f : -1.f, sy_ = (c & 1) ? 1.f : -1.f;
+                                    rr[c] = rcp_fast(D0 + sx_ * hd0 + sy_ * hd1);
+                                    const float uu = (Nu0 + sx_ * hu0 + sy_ * hu1) * rr[c];
+                                    umin = fminf(umin, uu);
+                                    umax = fmaxf(umax, uu);
+                                    bv[c] = sx_ * hv0 + sy_ * hv1;
+                                }
+                                const int ulo = max(0, (int)ceilf(umin - 1e-3f));
+                                const int uhi = min((int)P.nu - 1, (int)floorf(umax + 1e-3f));
+                                int vlo[kXB], vhi[kXB];
+                                float sk[kXB], zlo[kXB], zhi[kXB];
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    const float Nv = fmaf((float)k, dNv, Nv0);
+                                    float vmin = 3.0e38f, vmax = -3.0e38f;
+#pragma unroll
+                                    for (int c = 0; c < 4; ++c) {
+                                        const float v1 = (Nv + bv[c] - hv2) * rr[c], v2 = (Nv + bv[c] + hv2) * rr[c];
+                                        vmin = fminf(vmin, fminf(v1, v2));
+                                        vmax = fmaxf(vmax, fmaxf(v1, v2));
+                                    }
+                                    vlo[k] = live[k] ? max(0, (int)ceilf(vmin - 1e-3f)) : 1;
+                                    vhi[k] = live[k] ? min((int)P.nv - 1, (int)floorf(vmax + 1e-3f)) : 0;
+                                    // ray origin relative to the voxel's centre, z part: the slab's
+                                    // bounds -h - r0z and h - r0z
+                                    const float r0z = e.s.z - (Z0 + (float)k * vw * (float)kStride);
+                                    zlo[k] = -h - r0z;
+                                    zhi[k] = h - r0z;
+                                    sk[k] = 0.f;
+                                }
+                                const float r0x = e.s.x - X0, r0y = e.s.y - Y0;
+                                for (int iu = ulo; iu <= uhi; ++iu) {
+                                    const float dx = fmaf(e.u.x, (float)iu, e.d0.x);
+                                    const float dy = fmaf(e.u.y, (float)iu, e.d0.y);
+                                    const float duz = fmaf(e.u.z, (float)iu, e.d0.z);
+                                    float a_lo = 0.f, a_hi = 3.0e38f;
+                                    bool miss = false;
+                                    if (dx != 0.f) {
+                                        const float inv = rcp_fast(dx);
+                                        const float t1 = (-h - r0x) * inv, t2 = (h - r0x) * inv;
+                                        a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                        a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                    } else {
+                                        miss |= fabsf(r0x) > h;
+                                    }
+                                    if (dy != 0.f) {
+                                        const float inv = rcp_fast(dy);
+                                        const float t1 = (-h - r0y) * inv, t2 = (h - r0y) * inv;
+                                        a_lo = fmaxf(a_lo, fminf(t1, t2));
+                                        a_hi = fminf(a_hi, fmaxf(t1, t2));
+                                    } else {
+                                        miss |= fabsf(r0y) > h;
+                                    }
+                                    if (miss || !(a_hi > a_lo)) continue;  // the column's rays miss the voxels
+                                    const float dxy2 = dx * dx + dy * dy;
+                                    const float *pcol = pvw + iu * P.su;
+#pragma unroll
+                                    for (int k = 0; k < kXB; ++k) {
+                                        for (int iv = vlo[k]; iv <= vhi[k]; ++iv) {
+                                            const float dz = fmaf(e.v.z, (float)iv, duz);
+                                            float lo = a_lo, hi = a_hi;
+                                            if (dz != 0.f) {
+                                                const float inv = rcp_fast(dz);
+                                                const float t1 = zlo[k] * inv, t2 = zhi[k] * inv;
+                                                lo = fmaxf(lo, fminf(t1, t2));
+                                                hi = fminf(hi, fmaxf(t1, t2));
+                                            } else if (zlo[k] > 0.f || zhi[k] < 0.f) {
+                                                continue;  // |r0z| > h
+                                            }
+                                            if (!(hi > lo)) continue;
+                                            const float chord = (hi - lo) * sqrt_fast(dxy2 + dz * dz);
+                                            const float pv = P.all_ones ? 1.f : __ldg(pcol + iv * P.sv);
+                                            sk[k] = fmaf(pv, chord, sk[k]);
+                                        }
+                                    }
+                                }
+                                const float rD = rcp_fast(D0);
+                                const float fu = Nu0 * rD;
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    if (!live[k]) continue;
+                                    float s = sk[k];
+                                    if (needZ) s *= zpow(P, b, fmaf((float)k, dZ, Zb));
+                                    const float fv = fmaf((float)k, dNv, Nv0) * rD;
+                                    if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
+                                    acc[k] += s;
+                                }
+                            } else {
 #pragma unroll
                             for (int k = 0; k < kXB; ++k) {
                                 if (!live[k]) continue;
@@ -721,7 +841,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                                 miss |= fabsf(r0z) > h;
                                             }
                                             if (miss || !(a_hi > a_lo)) continue;
-                                            const float chord = (a_hi - a_lo) * sqrtf(dx * dx + dy * dy + dz * dz);
+                                            const float chord = (a_hi - a_lo) * sqrt_fast(dx * dx + dy * dy + dz * dz);
                                             const float pv = P.all_ones ? 1.f : __ldg(pvw + (iu * P.su + iv * P.sv));
                                             s = fmaf(pv, chord, s);
                                         }
@@ -730,6 +850,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                 }
                                 if (P.sep > 0.f && s != 0.f) s *= taper(b, fu, fv, P.inv_sep);
                                 acc[k] += s;
+                            }
                             }
                         } else {
                             // Fast modes: one branch-free pass over the thread's voxels;
@@ -974,15 +1095,17 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
 inline int bp_ord(const aprict_vol_desc *vd) { return vd->order == 0 ? (vd->nz == 1 && vd->ny > 1 ? 2 : 0) : 1; }
 
 // Host: whether ORD 3 (lanes and a thread's voxels along z) applies: the
-// fast nearest mode on a C-order volume tall enough to fill the 32 XB voxels
-// of a thread column, unless tuning knob 7 is 1, with a v stride below 2^30
-// elements (the gathers form their byte address as a 32 x 32-bit product).
-// Measured on a 256^3 volume with 360 views: nearest 9.82 -> 8.68 ms; bilinear
-// (27.4 vs 28.1 ms) and exact (114.6 vs 115.2 ms) keep ORD 0.
+// fast nearest mode, or the exact mode where exact_ok (one-scan calls), on a
+// C-order volume tall enough to fill the 32 XB voxels of a thread column,
+// unless tuning knob 7 is 1, with a v stride below 2^30 elements (the gathers
+// form their byte address as a 32 x 32-bit product). Measured on a 256^3
+// volume with 360 views: nearest 9.82 -> 8.68 ms; on 128^3 with 180 views,
+// exact 10.0 -> 7.1 ms (the column's x-y quantities shared); bilinear (27.4 vs
+// 28.1 ms) keeps ORD 0.
 inline bool bp_zlanes_ok(const aprict_vol_desc *vd, const aprict_proj_desc *pd, int xb,
-                         const aprict_backproject_config *cfg) {
+                         const aprict_backproject_config *cfg, bool exact_ok = false) {
     return bp_ord(vd) == 0 && ab_tuning_get(AB_TUNE_BP_ZLANES) != 1 && vd->nz >= 32u * (uint32_t)xb &&
-           pd->stride_v < (int64_t)1 << 30 && !cfg->exact && !cfg->approx_mode_direct_raycast &&
+           pd->stride_v < (int64_t)1 << 30 && (!cfg->exact || exact_ok) && !cfg->approx_mode_direct_raycast &&
            !cfg->approx_mode_linear_interpolate;
 }
 
@@ -1074,12 +1197,12 @@ inline int make_bp_params(const aprict_proj_spec *specs_dev, const aprict_proj_d
     const int knob = ab_tuning_get(AB_TUNE_BP_XB);
     const bool forced = force_xb == 2 || force_xb == 4 || force_xb == 8;
     xb = forced ? force_xb : (knob == 2 || knob == 4 || knob == 8 ? knob : default_xb(cfg->exact != 0));
-    const int ord = ord_out && bp_zlanes_ok(vd, pd, xb, cfg) ? 3 : bp_ord(vd);
+    const int ord = ord_out && bp_zlanes_ok(vd, pd, xb, cfg, true) ? 3 : bp_ord(vd);
     if (ord_out) *ord_out = ord;
     // z columns of 8 voxels per thread where the volume is tall enough (the
     // per-view work of a thread is shared by twice as many voxels: sirt256
     // 8.66 -> 8.35 ms), unless the caller or the knob chose
-    if (ord == 3 && !forced && knob == 0 && vd->nz >= 256u) xb = 8;
+    if (ord == 3 && !forced && knob == 0 && vd->nz >= 256u && !cfg->exact) xb = 8;
     const int kXB = xb;
     if (ord == 2) {  // slices: lanes along y, warps x XB along x
         P.gb[0] = (P.n[1] + 31) / 32;

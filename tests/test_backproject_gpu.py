@@ -238,3 +238,42 @@ def test_views_off_the_detector(case: str) -> None:
     v = Volume.zeros(SHAPE, voxwid=1.0)
     ScanBatch([v], [fp.ProjectionSet(pg, data=torch.from_numpy(projs).cuda())]).backproject(cfg, block=True)
     np.testing.assert_array_equal(v.as_numpy(), got)
+
+
+ZSHAPE = (24, 20, 70)  # tall enough (C order) for the z-column layout of the exact mode, with a partial column
+
+
+@pytest.mark.parametrize("case", ["exact", "exact-zpow", "exact-taper-mask", "exact-ones", "exact-supersample"])
+@pytest.mark.parametrize("geom", ["upright", "jittered"])
+def test_exact_z_columns_match_oracle(case: str, geom: str) -> None:
+    """The exact mode in the z-column layout: upright detectors take the path
+    that shares the column's x-y quantities, jittered (tilted) detectors the
+    per-voxel path of the same kernel; both against the FP64 oracle, and
+    against the brick layout (tuning knob 7 = 1) to FP32 rounding."""
+    from aprict_b200 import autotune
+
+    cfg = fp.ConfigBackproject(**CASES[case])
+    pg = circular(24, 120, 120, 0.537, 48, 84)
+    if geom == "jittered":
+        pg = jittered(np.random.default_rng(5), pg)
+    projs = _projs(pg, seed=3)
+    ps = fp.ProjectionSet(pg, data=torch.from_numpy(projs).cuda())
+
+    def run() -> np.ndarray:
+        v = Volume.zeros(ZSHAPE, voxwid=1.0)
+        fp.backproject(cfg, v, ps, block=True)
+        return v.as_numpy()
+
+    got = run()
+    autotune.apply({"bp_zlanes": 1})
+    try:
+        brick = run()
+    finally:
+        autotune.apply({})
+    corner = -np.array(ZSHAPE, np.float32) / 2
+    want = O.backproject(pg.to_proj_spec_array(), projs, ZSHAPE, cfg.contents, voxwid=1.0, corner=corner)
+    assert np.linalg.norm(want) > 0
+    err, err_b = rel_l2(got, want), rel_l2(got, brick)
+    print(f"{case} {geom}: rel L2 vs FP64 = {err:.2e}, vs brick layout = {err_b:.2e}")
+    assert err <= TOL
+    assert err_b <= 1e-6
