@@ -342,7 +342,8 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
     // one x layer per CTA: a thread's voxels then share x and y, so for views
     // whose detector u axis and normal have no z component (circular and
     // helical scans with an upright detector) the voxels share their depth and
-    // u coordinate, which are computed once per thread and view.
+    // u coordinate, which are computed once per warp and view (the fast modes)
+    // or once per thread and view (the exact mode).
     constexpr bool kZ = ORD == 3;
     constexpr int a0 = ORD == 0 || ORD == 3 ? 2 : (ORD == 1 ? 0 : 1);
     constexpr int a1 = ORD == 2 ? 2 : 1;
@@ -667,8 +668,8 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                 // vertical edges, the footprint's pixel columns and, per pixel
                                 // column, the x-y slab of its rays (whose x and y do not depend
                                 // on the row) are computed once per thread and view; per voxel
-                                // only the v extent and, per pixel, the z slab remain. The
-                                // arithmetic per quantity is the per-voxel path's.
+                                // only the v extent and, per pixel, the z slab remain, each by
+                                // the per-voxel path's formulas.
                                 const ab_bpview_exact e = sx[t];
                                 const float h = 0.5f * vw;
                                 const float hd0 = b.den.x * h, hd1 = b.den.y * h;
