@@ -341,6 +341,42 @@ AB_HD bool ab_siddon_gather(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3
     return true;
 }
 
+// The transpose of ab_siddon_gather: adds w * seg to vol[off] for every
+// segment of the ray (one atomic add per voxel crossed; zero-length segments
+// add nothing), with the same counted step loop and per-step arithmetic.
+#if defined(__CUDACC__)
+template <typename Off>
+__device__ __forceinline__ bool ab_siddon_scatter(ab_d3 o, ab_d3 e, const int n[3], const Off stride[3], float *vol,
+                                                  float w, bool *bad, int one = 1) {
+    ab_ray<Off> R;
+    if (!ab_siddon_setup<Off>(o, e, n, stride, R, bad)) return false;
+    bool ok = true;
+    const int N = ab_axis_count(R.t0x, R.dtx, R.tend, ok) + ab_axis_count(R.t0y, R.dty, R.tend, ok) +
+                  ab_axis_count(R.t0z, R.dtz, R.tend, ok);
+    if (!ok) {
+        *bad = true;
+        return false;
+    }
+    Off off = R.off;
+    float kx = 0.f, ky = 0.f, kz = 0.f;
+    float tx = R.t0x, ty = R.t0y, tz = R.t0z;
+    float t = 0.f;
+    for (int i = 0; i < N; ++i) {
+        const float tm = fminf(tx, fminf(ty, tz));
+        const float seg = tm - t;
+        if (seg > 0.f) atomicAdd(vol + off, seg * w);
+        t = tm;
+        if constexpr (sizeof(Off) == 4)
+            AB_SIDDON_ADVANCE_I32(R, off, kx, ky, kz, tx, ty, tz, tm, one);
+        else
+            AB_SIDDON_ADVANCE(R, off, kx, ky, kz, tx, ty, tz, tm);
+    }
+    const float seg = R.tend - t;  // the last segment ends at the exit
+    if (seg > 0.f) atomicAdd(vol + off, seg * w);
+    return true;
+}
+#endif
+
 // Kahan-compensated FP32 accumulator.
 struct ab_kahan {
     float s, c;

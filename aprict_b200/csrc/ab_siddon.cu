@@ -8,15 +8,6 @@ namespace {
 
 using namespace ab_fp;
 
-template <typename Off>
-struct ScatterVisit {
-    float *__restrict__ vol;
-    float w;
-    __device__ __forceinline__ void operator()(float seg, Off off) {
-        if (seg > 0.f) atomicAdd(vol + off, seg * w);
-    }
-};
-
 // Projector kernels over linear tile indices (used when the tile counts do
 // not fit a 3-D grid).
 template <typename Off, bool SS1>
@@ -61,7 +52,7 @@ template <typename Off>
 __global__ void __launch_bounds__(kThreads, 4)
     k_backproject_scatter(const aprict_proj_spec *__restrict__ specs, uint32_t n_views, uint32_t nu, uint32_t nv,
                           ab_pstrides ps, const float *__restrict__ projs, ab_grid<Off> g, float *vol, float svf,
-                          float mba, int ssu, int ssv, TileMap tm, uint32_t *status) {
+                          float mba, int ssu, int ssv, TileMap tm, uint32_t *status, int one) {
     int view, iu, iv;
     if (!block_tile(tm, n_views, blockIdx.x, view, iu, iv) || iu >= (int)nu || iv >= (int)nv) return;
     const int64_t o = (int64_t)view * ps.view + (int64_t)iu * ps.u + (int64_t)iv * ps.v;
@@ -78,8 +69,7 @@ __global__ void __launch_bounds__(kThreads, 4)
             const double fu = (double)iu - 0.5 + inv_su * (ku + 0.5);
             const double fv = (double)iv - 0.5 + inv_sv * (kv + 0.5);
             const ab_d3 dst = ab_to_grid(g, ab_pixel_pos(sp, fu, fv) * (double)svf);
-            ScatterVisit<Off> vis{vol, w};
-            ab_siddon<Off>(src, dst, g.n, g.stride, vis, &bad);
+            ab_siddon_scatter<Off>(src, dst, g.n, g.stride, vol, w, &bad, one);
         }
     }
     if (bad && status) atomicOr(status, APRICT_STATUS_NONFINITE);
@@ -125,11 +115,11 @@ extern "C" int aprict_b200_backproject_scatter(const aprict_proj_spec *specs_dev
     if (small_volume(vd)) {
         k_backproject_scatter<int32_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
             specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int32_t>(*vd), vol_dev,
-            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev, 1);
     } else {
         k_backproject_scatter<int64_t><<<(unsigned)nblocks, kThreads, 0, st>>>(
             specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, ab_make_grid<int64_t>(*vd), vol_dev,
-            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev);
+            cfg->shrink_volume_factor, cfg->multiply_before_adding, (int)cfg->ssu, (int)cfg->ssv, tm, status_dev, 1);
     }
     return ab_cuda_check(cudaGetLastError(), "backproject_scatter launch");
 }
