@@ -187,8 +187,10 @@ __device__ __forceinline__ bool brick_off_detector(const ab_bpview &b, const flo
 // projection of the box lies within the hull of its corners' projections
 // when all of them lie in front of the source; the FP32 coordinates of the
 // corners and of any voxel each carry at most the view's error bound, which
-// is below (1/2 - tie) / 1.5, so two bounds plus 1e-3 pixel are kept free.
-__device__ __forceinline__ bool brick_in_flat_box(const ab_bpview &b, const float lo[3], const float hi[3]) {
+// is below (1/2 - tie) / 1.5, so two bounds plus 1e-3 pixel are kept free
+// (plus `extra`: 1/2 keeps both bilinear taps of every voxel on the detector).
+__device__ __forceinline__ bool brick_in_flat_box(const ab_bpview &b, const float lo[3], const float hi[3],
+                                                  float extra = 0.f) {
     float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
     bool front = true;
 #pragma unroll
@@ -203,7 +205,7 @@ __device__ __forceinline__ bool brick_in_flat_box(const ab_bpview &b, const floa
         vmin = fminf(vmin, fv);
         vmax = fmaxf(vmax, fv);
     }
-    const float mu = (0.5f - b.tie_u) * (4.f / 3.f) + 1e-3f, mv = (0.5f - b.tie_v) * (4.f / 3.f) + 1e-3f;
+    const float mu = (0.5f - b.tie_u) * (4.f / 3.f) + 1e-3f + extra, mv = (0.5f - b.tie_v) * (4.f / 3.f) + 1e-3f + extra;
     return front && umin - mu >= -b.tap_ru && umax + mu <= b.tap_ru && vmin - mv >= -b.tap_rv &&
            vmax + mv <= b.tap_rv;
 }
@@ -400,13 +402,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
     // their slice, so they skip nothing and keep the plain loop (the skip's
     // per-view work measured 15 % on 64 fan-beam slices).
     constexpr bool kSkip = SKIP && !EXACT && ORD != 2;
-    // Interior bricks (nearest-pixel fast and direct-raycast modes): in a view
-    // that projects the whole brick into the detector's flat box, only
-    // near-tie pixel choices can need the second pass, and the voxels take a
-    // predicate-free pass (see the view loop). Not for slice stacks, whose
+    // Interior bricks (fast and direct-raycast modes, nearest or bilinear): in a
+    // view that projects the whole brick into the detector's flat box, only
+    // near-tie pixel choices can need the second pass (none with bilinear
+    // taps), and the voxels take a predicate-free pass (see the view loop).
+    // Not for slice stacks, whose
     // small bricks pay more for the per-view corner projections than the pass
     // saves (64 fan-beam slices: 1953 -> 1830 slices/s with it).
-    constexpr bool kInt = !EXACT && !BILIN && ORD != 2;
+    constexpr bool kInt = !EXACT && ORD != 2;
     // The brick's box relative to the volume centre (voxel faces, clipped to
     // the volume): every sub-sample of its voxels lies inside. Kept in shared
     // memory for the per-view off-detector test (ordered by the chunk loop's
@@ -568,7 +571,7 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                         if (kSkip) sm.off_det[t] = brick_off_detector(bt, sm.box, sm.box + 3, BILIN ? 0.5f : 0.f);
                         if (kInt)
                             sm.inner[t] = (uint8_t)(P.wide && bt.tie_u >= 0.25f && bt.tie_v >= 0.25f &&
-                                                    brick_in_flat_box(bt, sm.boxa, sm.boxa + 3));
+                                                    brick_in_flat_box(bt, sm.boxa, sm.boxa + 3, BILIN ? 0.5f : 0.f));
                         const float vws = vw * (float)kStride;
                         sm.sd[t] = make_float4((a2 == 0 ? bt.nu.x : (a2 == 1 ? bt.nu.y : bt.nu.z)) * vws,
                                                (a2 == 0 ? bt.nv.x : (a2 == 1 ? bt.nv.y : bt.nv.z)) * vws,
@@ -925,7 +928,42 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                     }
                                     }
                                 }
-                            } else if (kInt && sm.inner[t]) {
+                            } else if (kInt && BILIN && sm.inner[t]) {
+                                // Interior brick, bilinear: every voxel's four taps are on the
+                                // detector with taper weight 1 (the flat box less 1/2 pixel), so
+                                // they are loaded without bounds checks and nothing is deferred;
+                                // the interpolation is fetch_bilinear's, in the same order.
+                                const uint64_t vb = (uint64_t)(uintptr_t)pvw;
+                                const uint32_t su4 = 4u * (uint32_t)P.su, sv4 = 4u * (uint32_t)P.sv;
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    const float kf = (float)k;
+                                    const float D = fmaf(kf, dD, D0);
+                                    const float rD = rcp_fast(D);
+                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                    const float fv = fmaf(kf, dNv, Nv0) * rD;
+                                    float w = RAYCAST ? 1.f : rD * rD;
+                                    if (needZ) {
+                                        const float Zk = fmaf(kf, dZ, Zb);
+                                        w *= zpow(P, b, Zk);
+                                        if (RAYCAST && P.preset != 0)
+                                            w *= preset_weight(P.preset, P.val, X0 + (a2 == 0 ? kf * vw : 0.f) + P.c0[0],
+                                                               Y0 + P.c0[1], b.sxw, b.syw, Zk);
+                                    }
+                                    const float flu = floorf(fu), flv = floorf(fv);
+                                    const float fx = fu - flu, fy = fv - flv;
+                                    const float *p00 = reinterpret_cast<const float *>(
+                                        vb + (uint64_t)(uint32_t)(int)flu * su4 + (uint64_t)(uint32_t)(int)flv * sv4);
+                                    const float *p10 = reinterpret_cast<const float *>(reinterpret_cast<uintptr_t>(p00) + su4);
+                                    const float v00 = __ldg(p00), v01 = __ldg(reinterpret_cast<const float *>(
+                                                                      reinterpret_cast<uintptr_t>(p00) + sv4));
+                                    const float v10 = __ldg(p10), v11 = __ldg(reinterpret_cast<const float *>(
+                                                                      reinterpret_cast<uintptr_t>(p10) + sv4));
+                                    const float t1 = v00 * (1.f - fx) + v10 * fx;
+                                    const float t2 = v01 * (1.f - fx) + v11 * fx;
+                                    acc[k] = fmaf(t1 * (1.f - fy) + t2 * fy, w, acc[k]);
+                                }
+                            } else if (kInt && !BILIN && sm.inner[t]) {
                                 // Interior brick: every voxel's pixel is on the detector with
                                 // taper weight 1, so the pass has no predicates; it loads every
                                 // voxel's FP32-rounded pixel (dead voxels are never written) and
