@@ -472,6 +472,33 @@ struct TileMap {
     int tile_u, tile_v, ntu, ntv;
 };
 
+// Per view and shape, computed once per view (k_forbild_prep) instead of in
+// every detector tile: the pixel rectangle of the shape's bounding box
+// (all = 1: some corner is not in front of the source, keep for every tile;
+// kind 0 shapes are never kept) and the shape in the view's ray frame.
+struct QCull {
+    double u0, u1, v0, v1;
+    int keep_all, live;
+};
+
+__global__ void __launch_bounds__(128) k_forbild_prep(const aprict_proj_spec *__restrict__ specs, uint32_t view0,
+                                                      uint32_t nvw, const aprict_quadric *__restrict__ shapes,
+                                                      int n_shapes, QCull *cull, QView *qv) {
+    const int j = blockIdx.x * 128 + (int)threadIdx.x;
+    const uint32_t vi = blockIdx.y;
+    if (j >= n_shapes || vi >= nvw) return;
+    ViewGeom g;
+    view_geom(specs[view0 + vi], g);
+    const aprict_quadric &q = shapes[j];
+    QCull c{0.0, 0.0, 0.0, 0.0, 0, q.kind != 0};
+    const size_t o = (size_t)vi * (size_t)n_shapes + (size_t)j;
+    if (c.live) {
+        c.keep_all = !footprint(g, q, c.u0, c.u1, c.v0, c.v1);
+        make_qview(g, q, qv[o]);
+    }
+    cull[o] = c;
+}
+
 TileMap make_tiles(uint32_t nu, uint32_t nv) {
     TileMap t;
     t.tile_v = nv >= 16 ? 16 : 1;
@@ -493,7 +520,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_pr
                                                                ab_pstrides ps, float *out,
                                                                const aprict_quadric *__restrict__ shapes,
                                                                int n_shapes, float mba, int ssu, int ssv, TileMap tm,
-                                                               uint32_t view0, uint32_t *overflow) {
+                                                               uint32_t view0, uint32_t *overflow,
+                                                               const QCull *__restrict__ pcull,
+                                                               const QView *__restrict__ pqv) {
     extern __shared__ double smem_d[];
     QView *sel = reinterpret_cast<QView *>(smem_d);
     __shared__ int s_count;
@@ -541,7 +570,13 @@ __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_pr
                     __syncthreads();
                     const int j = c * kChunk + (int)threadIdx.x;
                     bool keep = false;
-                    if (threadIdx.x < kChunk && j < n_shapes && shapes[j].kind != 0) {
+                    if (pcull) {  // precomputed per view (k_forbild_prep)
+                        if (threadIdx.x < kChunk && j < n_shapes) {
+                            const QCull cr = pcull[(size_t)blockIdx.y * (size_t)n_shapes + (size_t)j];
+                            keep = cr.live && (cr.keep_all || (cr.u1 >= tu0 - 1e-6 && cr.u0 <= tu1 + 1e-6 &&
+                                                               cr.v1 >= tv0 - 1e-6 && cr.v0 <= tv1 + 1e-6));
+                        }
+                    } else if (threadIdx.x < kChunk && j < n_shapes && shapes[j].kind != 0) {
                         double u0, u1, v0, v1;
                         keep = !footprint(g, shapes[j], u0, u1, v0, v1) ||
                                (u1 >= tu0 - 1e-6 && u0 <= tu1 + 1e-6 && v1 >= tv0 - 1e-6 && v0 <= tv1 + 1e-6);
@@ -562,7 +597,10 @@ __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_pr
                     __syncthreads();
                     if (keep) {
                         const int pos = s_warp_pos[w] + __popc(bal & ((1u << lane) - 1u));
-                        make_qview(g, shapes[j], sel[pos]);
+                        if (pqv)
+                            sel[pos] = pqv[(size_t)blockIdx.y * (size_t)n_shapes + (size_t)j];
+                        else
+                            make_qview(g, shapes[j], sel[pos]);
                     }
                     __syncthreads();
                     cached_chunk = n_chunks == 1 ? c : -1;
@@ -642,15 +680,34 @@ extern "C" int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
     rc = ab_cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                        "project_forbild smem");
     if (rc != APRICT_OK) return rc;
-    for (uint32_t v0 = 0; v0 < pd->n_views; v0 += 65535u) {
-        const uint32_t nvw = pd->n_views - v0 < 65535u ? pd->n_views - v0 : 65535u;
+    // Views in groups whose per-(view, shape) records fit 256 MB of
+    // stream-ordered scratch; without scratch every tile derives them itself.
+    const size_t rec = sizeof(QCull) + sizeof(QView);
+    uint64_t per = (256ull << 20) / ((uint64_t)n_shapes * rec);
+    per = per < 1 ? 1 : (per > 65535u ? 65535u : per);
+    const uint32_t group = (uint32_t)(per < pd->n_views ? per : pd->n_views);
+    void *scratch = nullptr;
+    if (cudaMallocAsync(&scratch, (size_t)group * (size_t)n_shapes * rec, st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        scratch = nullptr;
+    }
+    QCull *cull = static_cast<QCull *>(scratch);
+    QView *qv = scratch ? reinterpret_cast<QView *>(cull + (size_t)group * (size_t)n_shapes) : nullptr;
+    for (uint32_t v0 = 0; v0 < pd->n_views && rc == APRICT_OK; v0 += group) {
+        const uint32_t nvw = pd->n_views - v0 < group ? pd->n_views - v0 : group;
+        if (scratch) {
+            k_forbild_prep<<<dim3((unsigned)((n_shapes + 127) / 128), nvw), 128, 0, st>>>(
+                specs_dev, v0, nvw, shapes_dev, (int)n_shapes, cull, qv);
+            rc = ab_cuda_check(cudaGetLastError(), "project_forbild prep launch");
+            if (rc != APRICT_OK) break;
+        }
         dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
         k<<<grid, kThreads, smem, st>>>(specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, shapes_dev,
-                                        (int)n_shapes, mba, (int)ssu, (int)ssv, tm, v0, overflow_dev);
+                                        (int)n_shapes, mba, (int)ssu, (int)ssv, tm, v0, overflow_dev, cull, qv);
         rc = ab_cuda_check(cudaGetLastError(), "project_forbild launch");
-        if (rc != APRICT_OK) return rc;
     }
-    return APRICT_OK;
+    if (scratch) cudaFreeAsync(scratch, st);
+    return rc;
 }
 
 // ---------------------------------------------------------------------------
