@@ -514,7 +514,11 @@ TileMap make_tiles(uint32_t nu, uint32_t nv) {
 // 720-view workload: 142.9 ms at 2 CTAs, 127.3 at 3, 113.4 at 4, 109.3 at 5,
 // 119.8 at 6 (96-shape chunks); 102.7 ms at 5 with 128-shape chunks, which
 // hold the 100 shapes in one chunk (warps wait at one barrier round, not two).
-template <int MODE>
+// PRE: the per-(view, shape) cull records and ray-frame shapes come from
+// k_forbild_prep (85.3 ms with them in the same kernel as the in-tile
+// derivation, 70.9 ms in a variant without it: fewer spills; 81.6 ms at 6
+// CTAs per SM).
+template <int MODE, bool PRE>
 __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_proj_spec *__restrict__ specs,
                                                                uint32_t n_views, uint32_t nu, uint32_t nv,
                                                                ab_pstrides ps, float *out,
@@ -570,13 +574,13 @@ __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_pr
                     __syncthreads();
                     const int j = c * kChunk + (int)threadIdx.x;
                     bool keep = false;
-                    if (pcull) {  // precomputed per view (k_forbild_prep)
+                    if (PRE) {  // precomputed per view (k_forbild_prep)
                         if (threadIdx.x < kChunk && j < n_shapes) {
                             const QCull cr = pcull[(size_t)blockIdx.y * (size_t)n_shapes + (size_t)j];
                             keep = cr.live && (cr.keep_all || (cr.u1 >= tu0 - 1e-6 && cr.u0 <= tu1 + 1e-6 &&
                                                                cr.v1 >= tv0 - 1e-6 && cr.v0 <= tv1 + 1e-6));
                         }
-                    } else if (threadIdx.x < kChunk && j < n_shapes && shapes[j].kind != 0) {
+                    } else if (threadIdx.x < kChunk && j < n_shapes && shapes[j].kind != 0) {  // derived here
                         double u0, u1, v0, v1;
                         keep = !footprint(g, shapes[j], u0, u1, v0, v1) ||
                                (u1 >= tu0 - 1e-6 && u0 <= tu1 + 1e-6 && v1 >= tv0 - 1e-6 && v0 <= tv1 + 1e-6);
@@ -597,7 +601,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_pr
                     __syncthreads();
                     if (keep) {
                         const int pos = s_warp_pos[w] + __popc(bal & ((1u << lane) - 1u));
-                        if (pqv)
+                        if constexpr (PRE)
                             sel[pos] = pqv[(size_t)blockIdx.y * (size_t)n_shapes + (size_t)j];
                         else
                             make_qview(g, shapes[j], sel[pos]);
@@ -676,10 +680,15 @@ extern "C" int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
     const ab_pstrides ps{pd->stride_view, pd->stride_u, pd->stride_v};
     const size_t smem = (size_t)kChunk * sizeof(QView);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    auto *k = mode == 0 ? k_project_forbild<0> : (mode == 1 ? k_project_forbild<1> : k_project_forbild<2>);
-    rc = ab_cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                       "project_forbild smem");
-    if (rc != APRICT_OK) return rc;
+    auto *kd = mode == 0 ? k_project_forbild<0, false>
+                         : (mode == 1 ? k_project_forbild<1, false> : k_project_forbild<2, false>);
+    auto *kp = mode == 0 ? k_project_forbild<0, true>
+                         : (mode == 1 ? k_project_forbild<1, true> : k_project_forbild<2, true>);
+    for (auto *kk : {kd, kp}) {
+        rc = ab_cuda_check(cudaFuncSetAttribute(kk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                           "project_forbild smem");
+        if (rc != APRICT_OK) return rc;
+    }
     // Views in groups whose per-(view, shape) records fit 256 MB of
     // stream-ordered scratch; without scratch every tile derives them itself.
     const size_t rec = sizeof(QCull) + sizeof(QView);
@@ -702,8 +711,9 @@ extern "C" int aprict_b200_project_forbild(const aprict_proj_spec *specs_dev, co
             if (rc != APRICT_OK) break;
         }
         dim3 grid((unsigned)(tm.ntu * tm.ntv), nvw);
-        k<<<grid, kThreads, smem, st>>>(specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev, shapes_dev,
-                                        (int)n_shapes, mba, (int)ssu, (int)ssv, tm, v0, overflow_dev, cull, qv);
+        (scratch ? kp : kd)<<<grid, kThreads, smem, st>>>(specs_dev, pd->n_views, pd->nu, pd->nv, ps, projs_dev,
+                                                          shapes_dev, (int)n_shapes, mba, (int)ssu, (int)ssv, tm, v0,
+                                                          overflow_dev, cull, qv);
         rc = ab_cuda_check(cudaGetLastError(), "project_forbild launch");
     }
     if (scratch) cudaFreeAsync(scratch, st);
