@@ -298,6 +298,7 @@ struct BPSmem {
     int vcount;               // views of the chunk whose brick projection reaches the detector
     uint8_t off_det[kChunk];  // per view: the whole brick projects beyond one detector edge
     uint8_t zinv[kChunk];     // per view: depth and u do not change along z (ORD 3 shares them)
+    uint8_t vzero[kChunk];    // per view (slice stacks): one detector row, v form identically zero
     uint8_t vlist[kChunk];    // those views' indices in the chunk, in order
     uint16_t q[EXACT ? 1 : kWarps][EXACT ? 1 : kQCap];
     // Nearest mode, z-column layout: per warp, the warp-uniform part of 32
@@ -586,6 +587,14 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                             sm.zinv[t] = (uint8_t)(kZ && kNear && bt.den.z == 0.f && bt.nu.z == 0.f &&
                                                    (!needZ || bt.zl.z == 0.f) && svd[t].nu[2] == 0.0 &&
                                                    svd[t].den[2] == 0.0);
+                        // A fan-beam slice: the v form vanishes in the slice plane (its x, y
+                        // and constant coefficients are exact zeros), and with one z layer
+                        // and no z sub-samples every sample lies in that plane (z = 0
+                        // relative to the volume centre, exactly): every voxel projects
+                        // onto row 0 of the one-row detector exactly.
+                        if constexpr (ORD == 2)
+                            sm.vzero[t] = (uint8_t)(P.nv == 1u && P.n[2] == 1 && P.ssz == 1 && bt.nv.x == 0.f &&
+                                                    bt.nv.y == 0.f && bt.nv.w == 0.f);
                     }
                     __syncthreads();
                     // The chunk's views whose projection of the brick reaches the
@@ -927,6 +936,39 @@ __device__ __forceinline__ void bp_brick(const BPParams &P, uint32_t brick,
                                         pending |= (live[k] && !fast && !outside) ? 1u << k : 0u;
                                     }
                                     }
+                                }
+                            } else if (ORD == 2 && !BILIN && sm.vzero[t]) {
+                                // Fan-beam slice: one detector row and a v form that is zero
+                                // at every point, so every voxel projects onto row 0 exactly
+                                // (v = 0 = the row centre, no tie, inside the flat box in v);
+                                // only u is computed, by the same steps as the general loop.
+                                const uint32_t offu0 = 0u - 0x4B400000u * (uint32_t)P.su;
+#pragma unroll
+                                for (int k = 0; k < kXB; ++k) {
+                                    const float kf = (float)k;
+                                    const float D = fmaf(kf, dD, D0);
+                                    const float rD = rcp_fast(D);
+                                    const float fu = fmaf(kf, dNu, Nu0) * rD;
+                                    float w = RAYCAST ? 1.f : rD * rD;
+                                    if (needZ) {
+                                        const float Zk = fmaf(kf, dZ, Zb);
+                                        w *= zpow(P, b, Zk);
+                                        if (RAYCAST && P.preset != 0)
+                                            w *= preset_weight(P.preset, P.val, X0 + (a2 == 0 ? kf * vw : 0.f) + P.c0[0],
+                                                               Y0 + P.c0[1], b.sxw, b.syw, Zk);
+                                    }
+                                    const float au = fabsf(fu - b.cu0);
+                                    const bool outside = kSkip && au > b.out_ru;
+                                    const float tu = __fadd_rn(fu, kMagic);
+                                    const float du = __fsub_rn(fu, __fsub_rn(tu, kMagic));
+                                    const bool fast = au <= b.tap_ru && fabsf(du) <= b.tie_u;
+                                    const int off = (int)((uint32_t)__float_as_int(tu) * (uint32_t)P.su + offu0);
+                                    float pv = 0.f;
+                                    if (live[k] && fast) pv = __ldg(pvw + off);
+                                    acc[k] = fmaf(pvp[k], wp[k], acc[k]);
+                                    pvp[k] = pv;
+                                    wp[k] = w;
+                                    pending |= (live[k] && !fast && !outside) ? 1u << k : 0u;
                                 }
                             } else if (kInt && BILIN && sm.inner[t]) {
                                 // Interior brick, bilinear: every voxel's four taps are on the
