@@ -219,6 +219,210 @@ __global__ void __launch_bounds__(kGThreads, BILIN ? 3 : 4) k_backproject_gbc(co
     if (value2 != 0.f) G.vol2[o] = value2 * m + G.vol2[o];
 }
 
+// Z-column layout for C-order volumes: the 32 lanes of a warp and each
+// thread's kGZ voxels lie along z (voxel k of a lane 32 k further), warps
+// along y, one x layer per CTA. For a view whose detector u axis and normal
+// have no z component (the GBC's cylindrical scans) the thread's voxels share
+// x and y, and with them everything horizontal: the depth and its
+// reciprocal, u (the pixel column or the bilinear columns and their weight),
+// the horizontal distance ell, the horizontal angle's cosine c, its window,
+// and the weight's factor c / max(1e-9, c^2 + (c - ell)^2). Per voxel only
+// the elevation (its cosine cubed and window) and v remain. Other views take
+// the per-voxel formulas of k_backproject_gbc.
+constexpr int kGZ = 4;
+
+template <bool BILIN>
+__global__ void __launch_bounds__(kGThreads, BILIN ? 3 : 4) k_backproject_gbc_z(const ab_bp::BPParams P, const GbcParams G,
+                                                                 int gb0, int gb1) {
+    using namespace ab_bp;
+    __shared__ ab_bpview sv[kGChunk];
+    __shared__ ab_bpview_d svd[BILIN ? 1 : kGChunk];
+    __shared__ float ssrc[kGChunk][4];  // source x, y, z, 1 / |(x, y)|
+    __shared__ uint8_t szinv[kGChunk];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int b0 = (int)(blockIdx.x % (unsigned)gb0), b1 = (int)((blockIdx.x / (unsigned)gb0) % (unsigned)gb1);
+    const int ix = (int)(blockIdx.x / ((unsigned)gb0 * (unsigned)gb1));
+    const int iy = b1 * 8 + warp, iz0 = b0 * 32 * kGZ + lane;
+    const bool col_live = iy < P.n[1];
+    bool live[kGZ];
+#pragma unroll
+    for (int k = 0; k < kGZ; ++k) live[k] = col_live && iz0 + 32 * k < P.n[2];
+    const float vw = P.voxwid;
+    const float offs[3] = {1.f / (float)P.ssx, 1.f / (float)P.ssy, 1.f / (float)P.ssz};
+    const int n_sub = P.ssx * P.ssy * P.ssz;
+    float acc[kGZ], acc2[kGZ];
+#pragma unroll
+    for (int k = 0; k < kGZ; ++k) acc[k] = acc2[k] = 0.f;
+
+    for (uint32_t v0 = 0; v0 < P.n_views; v0 += kGChunk) {
+        const int cn = (int)min((uint32_t)kGChunk, P.n_views - v0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cn; t += kGThreads) {
+            const ab_d3 c0d{P.cornerd[0] + 0.5 * P.vwd * P.n[0], P.cornerd[1] + 0.5 * P.vwd * P.n[1],
+                            P.cornerd[2] + 0.5 * P.vwd * P.n[2]};
+            const aprict_proj_spec sp = P.specs[v0 + t];
+            const double hext[3] = {(0.5 * P.n[0] + 1.0) * P.vwd, (0.5 * P.n[1] + 1.0) * P.vwd,
+                                    (0.5 * P.n[2] + 1.0) * P.vwd};
+            if (!ab_derive_bpview(sp, c0d, vw, 0.f, hext, sv[t], BILIN ? nullptr : &svd[t]) && P.status)
+                atomicOr(P.status, APRICT_STATUS_BAD_GEOMETRY);
+            ssrc[t][0] = sp.source_pos.x;
+            ssrc[t][1] = sp.source_pos.y;
+            ssrc[t][2] = sp.source_pos.z;
+            ssrc[t][3] = rsqrtf(sp.source_pos.x * sp.source_pos.x + sp.source_pos.y * sp.source_pos.y);
+            const ab_bpview &bt = sv[t];
+            szinv[t] = (uint8_t)(bt.den.z == 0.f && bt.nu.z == 0.f && (BILIN || (svd[t].nu[2] == 0.0 && svd[t].den[2] == 0.0)));
+        }
+        __syncthreads();
+        if (!__any_sync(0xffffffffu, col_live && live[0])) continue;  // warp-uniform
+        for (int isub = 0; isub < n_sub; ++isub) {
+            const int sidx[3] = {isub / (P.ssy * P.ssz), (isub / P.ssz) % P.ssy, isub % P.ssz};
+            float fsub[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) fsub[a] = -0.5f + offs[a] * (0.5f + (float)sidx[a]);
+            const int idv[2] = {ix, iy};
+            float rel[2], wp[2];
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                rel[a] = ((float)idv[a] + 0.5f - 0.5f * (float)P.n[a]) * vw + fsub[a] * vw;
+                wp[a] = (G.pos000[a] + (float)idv[a] * vw) + fsub[a] * vw;
+            }
+            float relz[kGZ], wpz[kGZ];
+#pragma unroll
+            for (int k = 0; k < kGZ; ++k) {
+                const int iz = iz0 + 32 * k;
+                relz[k] = ((float)iz + 0.5f - 0.5f * (float)P.n[2]) * vw + fsub[2] * vw;
+                wpz[k] = (G.pos000[2] + (float)iz * vw) + fsub[2] * vw;
+            }
+            float s[kGZ], s2[kGZ];
+#pragma unroll
+            for (int k = 0; k < kGZ; ++k) s[k] = s2[k] = 0.f;
+            for (int t = 0; t < cn; ++t) {
+                const ab_bpview &b = sv[t];
+                const float sx = ssrc[t][0], sy = ssrc[t][1], sz = ssrc[t][2], inv_ls = ssrc[t][3];
+                const float *pvw = P.projs + (int64_t)(v0 + t) * P.stride_view;
+                if (szinv[t]) {
+                    // horizontal: shared by the thread's voxels
+                    const float rx = wp[0] - sx, ry = wp[1] - sy;
+                    const float q = rx * rx + ry * ry;
+                    const float rq = rsqrtf(q);
+                    const float ell = q > 0.f ? q * rq * G.inv_R : 0.f;
+                    const float c = fmaxf(0.f, fminf(1.f, fabsf((rx * sx + ry * sy) * inv_ls * rq)));
+                    const float d = c - ell;
+                    const float ac = __fdividef(c, fmaxf(1e-9f, c * c + d * d)) *
+                                     soft_of_sin2(fmaxf(0.f, 1.f - c * c), G.soft.h);
+                    const float rD = rcp_fast(dot4(b.den, rel[0], rel[1], relz[0]));
+                    const float fu = dot4(b.nu, rel[0], rel[1], relz[0]) * rD;
+                    // u: the pixel column (nearest) or the two columns and their weight (bilinear)
+                    int iu = -1, i0 = 0;
+                    float fx = 0.f;
+                    bool ucol = false;
+                    if (BILIN) {
+                        ucol = !(fu <= -1.f || fu >= (float)P.nu);
+                        i0 = (int)floorf(fu);
+                        fx = fu - (float)i0;
+                    } else {
+                        float du;
+                        iu = round_index(fu, -2.f, P.fnu1, du);
+                        if (fabsf(du) > b.tie_u) {
+                            const VoxRef vr{((double)ix + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                            ((double)iy + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd, 0.0};
+                            iu = refine_index(svd[BILIN ? 0 : t].nu, svd[BILIN ? 0 : t].den, vr, iu, du);
+                        }
+                        ucol = (unsigned)iu < P.nu;
+                    }
+#pragma unroll
+                    for (int k = 0; k < kGZ; ++k) {
+                        const float zr = (wpz[k] - sz) * G.inv_R;
+                        const float h2 = ell * ell + zr * zr;
+                        const float ih = rsqrtf(h2);
+                        const float cos_el = h2 > 0.f ? ell * ih : 1.f;
+                        const float sin_el = h2 > 0.f ? fabsf(zr) * ih : 0.f;
+                        const float w = cos_el * cos_el * cos_el * ac * soft_of_sin(sin_el, sin_el * sin_el, G.soft.v);
+                        s2[k] += w;
+                        if (w == 0.f || !ucol) continue;
+                        const float fv = dot4(b.nv, rel[0], rel[1], relz[k]) * rD;
+                        float pv;
+                        if (BILIN) {
+                            if (fv <= -1.f || fv >= (float)P.nv) continue;
+                            const int j0 = (int)floorf(fv);
+                            const float fy = fv - (float)j0;
+                            auto get = [&](int i, int j) -> float {
+                                if (i < 0 || i >= (int)P.nu || j < 0 || j >= (int)P.nv) return 0.f;
+                                return __ldg(pvw + (i * P.su + j * P.sv));
+                            };
+                            const float v00 = get(i0, j0), v01 = get(i0, j0 + 1), v10 = get(i0 + 1, j0),
+                                        v11 = get(i0 + 1, j0 + 1);
+                            const float t1 = v00 * (1.f - fx) + v10 * fx;
+                            const float t2 = v01 * (1.f - fx) + v11 * fx;
+                            pv = t1 * (1.f - fy) + t2 * fy;
+                        } else {
+                            float dv;
+                            int iv = round_index(fv, -2.f, P.fnv1, dv);
+                            if (fabsf(dv) > b.tie_v) {
+                                const VoxRef vr{((double)ix + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                ((double)iy + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                ((double)(iz0 + 32 * k) + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) *
+                                                    P.vwd};
+                                iv = refine_index(svd[BILIN ? 0 : t].nv, svd[BILIN ? 0 : t].den, vr, iv, dv);
+                            }
+                            pv = (unsigned)iv < P.nv ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
+                        }
+                        s[k] = fmaf(pv, w, s[k]);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < kGZ; ++k) {
+                        const float w = gbc_weight(G.inv_R, wp[0], wp[1], wpz[k], sx, sy, sz, inv_ls, G.soft);
+                        s2[k] += w;
+                        if (w == 0.f) continue;
+                        const float rD = rcp_fast(dot4(b.den, rel[0], rel[1], relz[k]));
+                        const float fu = dot4(b.nu, rel[0], rel[1], relz[k]) * rD;
+                        const float fv = dot4(b.nv, rel[0], rel[1], relz[k]) * rD;
+                        float pv;
+                        if (BILIN) {
+                            pv = fetch_bilinear(P, pvw, fu, fv);
+                        } else {
+                            float du, dv;
+                            int iu = round_index(fu, -2.f, P.fnu1, du);
+                            int iv = round_index(fv, -2.f, P.fnv1, dv);
+                            const bool tu = fabsf(du) > b.tie_u, tv = fabsf(dv) > b.tie_v;
+                            if (tu || tv) {
+                                const VoxRef vr{((double)ix + 0.5 + (double)fsub[0] - 0.5 * P.n[0]) * P.vwd,
+                                                ((double)iy + 0.5 + (double)fsub[1] - 0.5 * P.n[1]) * P.vwd,
+                                                ((double)(iz0 + 32 * k) + 0.5 + (double)fsub[2] - 0.5 * P.n[2]) *
+                                                    P.vwd};
+                                const ab_bpview_d &cd = svd[BILIN ? 0 : t];
+                                if (tu) iu = refine_index(cd.nu, cd.den, vr, iu, du);
+                                if (tv) iv = refine_index(cd.nv, cd.den, vr, iv, dv);
+                            }
+                            const bool inb = (unsigned)iu < P.nu && (unsigned)iv < P.nv;
+                            pv = inb ? __ldg(pvw + (iu * P.su + iv * P.sv)) : 0.f;
+                        }
+                        s[k] = fmaf(pv, w, s[k]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kGZ; ++k) {
+                acc[k] += s[k];
+                acc2[k] += s2[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kGZ; ++k) {
+        if (!live[k]) continue;
+        const float value = n_sub == 1 ? acc[k] : acc[k] / (float)n_sub;
+        const float value2 = n_sub == 1 ? acc2[k] : acc2[k] / (float)n_sub;
+        if (value == 0.f && value2 == 0.f) continue;  // the reference writes neither (:1068-1075)
+        const int64_t o = (int64_t)ix * P.vs[0] + (int64_t)iy * P.vs[1] + (int64_t)(iz0 + 32 * k) * P.vs[2];
+        const float m = P.mult ? P.mult[o] : 1.f;
+        if (value != 0.f) P.vol[o] = value * m + P.vol[o];
+        if (value2 != 0.f) G.vol2[o] = value2 * m + G.vol2[o];
+    }
+}
+
 // Expected GBC weight sum at radius r (units of R) over a perfect cylindrical
 // source locus: sum over num_z heights z in [0, tan(vartheta_v) (1 + r_max)]
 // (the first with weight 1/2) and num_ang source angles t in [0, pi) of the
@@ -476,10 +680,19 @@ extern "C" int aprict_b200_backproject_gbc(const aprict_proj_spec *specs_dev, co
     if (blocks > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const int order_f = vd->order != 0;
-    if (cfg->approx_mode_linear_interpolate)
+    if (!order_f) {  // C order: z columns (see k_backproject_gbc_z)
+        const int64_t gb0 = ((int64_t)vd->nz + 32 * kGZ - 1) / (32 * kGZ), gb1 = ((int64_t)vd->ny + 7) / 8;
+        const int64_t zblocks = gb0 * gb1 * (int64_t)vd->nx;
+        if (zblocks > 0x7fffffffLL) return ab_fail(APRICT_ERR_TOO_LARGE, "volume too large for the grid");
+        if (cfg->approx_mode_linear_interpolate)
+            k_backproject_gbc_z<true><<<(unsigned)zblocks, kGThreads, 0, st>>>(P, G, (int)gb0, (int)gb1);
+        else
+            k_backproject_gbc_z<false><<<(unsigned)zblocks, kGThreads, 0, st>>>(P, G, (int)gb0, (int)gb1);
+    } else if (cfg->approx_mode_linear_interpolate) {
         k_backproject_gbc<true><<<(unsigned)blocks, kGThreads, 0, st>>>(P, G, order_f);
-    else
+    } else {
         k_backproject_gbc<false><<<(unsigned)blocks, kGThreads, 0, st>>>(P, G, order_f);
+    }
     return ab_cuda_check(cudaGetLastError(), "backproject_gbc launch");
 }
 
