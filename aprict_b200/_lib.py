@@ -54,6 +54,15 @@ SIGNATURES: dict[str, tuple[object, list[object]]] = {
             ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
         ],
     ),
+    "aprict_b200_ramp_fft_tables_bytes": (ctypes.c_int64, [ctypes.c_int64]),
+    "aprict_b200_ramp_fft_tables": (_c_int, [_c_void_p, ctypes.c_int64, _c_void_p, _c_void_p]),
+    "aprict_b200_ramp_filter_fft": (
+        _c_int,
+        [
+            _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+            ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _c_void_p,
+        ],
+    ),
     "aprict_b200_vol_div_softzero": (
         _c_int, [_c_void_p, _c_void_p, _c_void_p, ctypes.c_int64, ctypes.c_float, _c_void_p],
     ),

@@ -4,9 +4,10 @@ The reference filters a chunk of projections by zero-padding every detector
 row to next_fast_len(2 nu - 1), running cuFFT R2C, multiplying by the tap
 spectrum (complex128) and C2R (src/aprict/cb/ramp_filter.py:83-240), after a
 cosine weight per pixel (:407-449, applied at :685-689). That is a linear
-convolution, evaluated here directly by ``aprict_b200_ramp_filter`` (a
-shared-memory convolution kernel), one launch for the whole projection stack
-with the weights fused into the staging of each row.
+convolution, evaluated here in one launch for the whole projection stack with
+the weights fused into the staging of each row: by a shared-memory FFT
+(``aprict_b200_ramp_filter_fft``, from tables built once per filter) for rows
+of 128 to 2048 samples, else directly (``aprict_b200_ramp_filter``).
 
 ``FBPFilterer`` also filters along tilted lines for the cone-cylinder FBP
 (:577-886): each projection is padded to a wider frame, rotated by a random
@@ -69,6 +70,21 @@ class RampFilterer:
             self._taps_host.append(h)
             self._odd.append(ramp_kernels.odd_only(h))
             self._taps.append(torch.from_numpy(h.astype(np.float32)).cuda())
+        # Rows of 128 to 2048 samples are filtered by FFT from tables (kernel
+        # spectrum and twiddles) built here once per filter, as the reference
+        # keeps each filter's spectrum (ramp_filter.py:83-137); other lengths by
+        # the direct convolution of the taps.
+        lib = _lib.lib()
+        nbytes = int(lib.aprict_b200_ramp_fft_tables_bytes(nu))
+        self._fft_tables: list[torch.Tensor | None] = []
+        for t in self._taps:
+            tab = None
+            if nbytes > 0:
+                tab = torch.empty(nbytes, dtype=torch.uint8, device=t.device)
+                _lib.check(lib.aprict_b200_ramp_fft_tables(t.data_ptr(), nu, tab.data_ptr(), _stream()), "ramp_fft_tables")
+            self._fft_tables.append(tab)
+        self._tables_ready = torch.cuda.Event()
+        self._tables_ready.record()
 
     @property
     def num_kerns(self) -> int:
@@ -104,15 +120,26 @@ class RampFilterer:
                 raise ValueError(msg)
             wptr, (wsu, wsv) = weights.data_ptr(), weights.stride()
         din = _desc(data)
-        for taps, odd, out in zip(self._taps, self._odd, outs):
+        lib = _lib.lib()
+        torch.cuda.current_stream().wait_event(self._tables_ready)
+        for taps, odd, tab, out in zip(self._taps, self._odd, self._fft_tables, outs):
             dout = _desc(out)
-            _lib.check(
-                _lib.lib().aprict_b200_ramp_filter(
-                    _lib.ptr(din), data.data_ptr(), _lib.ptr(dout), out.data_ptr(), taps.data_ptr(), int(odd),
-                    wptr, wsu, wsv, float(scale), _stream(),
-                ),
-                "ramp_filter",
-            )
+            if tab is not None:
+                _lib.check(
+                    lib.aprict_b200_ramp_filter_fft(
+                        _lib.ptr(din), data.data_ptr(), _lib.ptr(dout), out.data_ptr(), tab.data_ptr(),
+                        wptr, wsu, wsv, float(scale), _stream(),
+                    ),
+                    "ramp_filter_fft",
+                )
+            else:
+                _lib.check(
+                    lib.aprict_b200_ramp_filter(
+                        _lib.ptr(din), data.data_ptr(), _lib.ptr(dout), out.data_ptr(), taps.data_ptr(), int(odd),
+                        wptr, wsu, wsv, float(scale), _stream(),
+                    ),
+                    "ramp_filter",
+                )
         return outs
 
     def filter_bulk_axis1_stream(self, arr: torch.Tensor, block: bool = True):  # noqa: ANN201

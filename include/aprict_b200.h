@@ -248,6 +248,24 @@ APRICT_API int aprict_b200_ramp_filter(const aprict_proj_desc *in, const float *
                                        int odd_taps_only, const float *weights_dev, int64_t w_stride_u,
                                        int64_t w_stride_v, float scale, aprict_stream_t stream);
 
+/* The same convolution by FFT, from tables built once per filter (the
+ * reference's RampFilterer keeps the kernel spectrum, ramp_filter.py:83-137):
+ * rows zero-padded to N = 2^p >= 2 nu - 1, two rows per complex transform,
+ * forward transform in FP64, inverse in FP32. For 128 <= nu <= 2048.
+ *   aprict_b200_ramp_fft_tables_bytes: bytes of the tables for rows of nu
+ *       samples (32 N), 0 where nu is outside the FFT range
+ *   aprict_b200_ramp_fft_tables: builds them from taps_dev (2*nu-1 floats)
+ *       into tables_dev (16-byte aligned), enqueued on stream
+ *   aprict_b200_ramp_filter_fft: aprict_b200_ramp_filter with the filter
+ *       given by tables built for the same nu; same arguments otherwise */
+APRICT_API int64_t aprict_b200_ramp_fft_tables_bytes(int64_t nu);
+APRICT_API int aprict_b200_ramp_fft_tables(const float *taps_dev, int64_t nu, void *tables_dev,
+                                           aprict_stream_t stream);
+APRICT_API int aprict_b200_ramp_filter_fft(const aprict_proj_desc *in, const float *in_dev,
+                                           const aprict_proj_desc *out, float *out_dev, const void *tables_dev,
+                                           const float *weights_dev, int64_t w_stride_u, int64_t w_stride_v,
+                                           float scale, aprict_stream_t stream);
+
 /* Rotated bilinear resampling of a projection stack: the per-projection
  * rotations of the cone-cylinder FBP filter with its padding, weight mask,
  * letterbox and crop (FBPFilterer.filter_bulk_axis1_stream,

@@ -147,6 +147,30 @@ def test_volops_validation() -> None:
     assert lib.aprict_b200_vol_softmask_cylinder(_fake(), _lib.ptr(vd), ctypes.c_float(1.5), None) == 1
 
 
+def test_ramp_fft_tables_validate_on_the_host() -> None:
+    lib = _lib.lib()
+    # 32 bytes per point of the transform, N = 2^p >= 2 nu - 1, for 128 <= nu <= 2048
+    assert lib.aprict_b200_ramp_fft_tables_bytes(127) == 0
+    assert lib.aprict_b200_ramp_fft_tables_bytes(2049) == 0
+    assert lib.aprict_b200_ramp_fft_tables_bytes(128) == 32 * 256
+    assert lib.aprict_b200_ramp_fft_tables_bytes(129) == 32 * 512
+    assert lib.aprict_b200_ramp_fft_tables_bytes(1024) == 32 * 2048
+    assert lib.aprict_b200_ramp_fft_tables_bytes(2048) == 32 * 4096
+    assert lib.aprict_b200_ramp_fft_tables(_fake(), 100, _fake(), None) == 2
+    assert lib.aprict_b200_ramp_fft_tables(None, 256, _fake(), None) == 1
+    assert lib.aprict_b200_ramp_fft_tables(_fake(), 256, _fake() + 8, None) == 1
+    din = _lib.proj_desc((3, 300, 2), (600, 2, 1))
+    dout = _lib.proj_desc((3, 300, 3), (900, 3, 1))
+    dshort = _lib.proj_desc((3, 100, 2), (200, 2, 1))
+    args = (None, 0, 0, ctypes.c_float(1.0), None)
+    src, dst = _fake(), _fake() + (1 << 24)
+    assert lib.aprict_b200_ramp_filter_fft(_lib.ptr(din), src, _lib.ptr(dout), dst, _fake(), *args) == 1
+    assert lib.aprict_b200_ramp_filter_fft(_lib.ptr(din), src, _lib.ptr(din), src, _fake(), *args) == 1
+    assert lib.aprict_b200_ramp_filter_fft(_lib.ptr(dshort), src, _lib.ptr(dshort), dst, _fake(), *args) == 2
+    assert lib.aprict_b200_ramp_filter_fft(_lib.ptr(din), src, _lib.ptr(din), dst, None, *args) == 1
+    assert lib.aprict_b200_ramp_filter_fft(_lib.ptr(din), src, _lib.ptr(din), dst, _fake() + 8, *args) == 1
+
+
 def test_tuning_knobs_validate_and_round_trip() -> None:
     lib = _lib.lib()
     saved = [lib.aprict_b200_get_tuning(k) for k in range(8)]

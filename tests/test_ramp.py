@@ -128,3 +128,37 @@ def test_gpu_filter_strided_views() -> None:
     v = view.cpu().numpy()
     want = np.stack([np.stack([conv_same_fp64(v[i, :, j], taps) for j in range(3)], -1) for i in range(3)])
     assert np.linalg.norm(out.cpu().numpy() - want) / np.linalg.norm(want) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nu", [127, 128, 129, 257, 438, 1000, 2048, 2049])
+@pytest.mark.parametrize("layout", ["u_rows", "v_rows", "strided"])
+def test_gpu_filter_sizes_and_layouts(nu: int, layout: str) -> None:
+    """Rows of 128 to 2048 samples take the FFT convolution (FP64 forward
+    transform, two rows per complex signal), shorter and longer ones the direct
+    convolution: both against the FP64 convolution, for rows contiguous along u
+    or v, strided views, an odd row count (the last complex signal carries one
+    row) and asymmetric taps (Hilbert at half-pixel offset)."""
+    import torch
+
+    from aprict_b200.cb.ramp_filter import RampFilterer
+
+    rng = np.random.default_rng(nu + len(layout))
+    m, nv = 3, 5
+    if layout == "u_rows":
+        data = torch.from_numpy(rng.random((m, nv, nu)).astype(np.float32)).cuda().permute(0, 2, 1)
+    elif layout == "v_rows":
+        data = torch.from_numpy(rng.random((m, nu, nv)).astype(np.float32)).cuda()
+    else:
+        big = torch.from_numpy(rng.random((2 * m, nu, 2 * nv + 1)).astype(np.float32)).cuda()
+        data = big[::2, :, 1::2]
+    w = torch.from_numpy(rng.random((nu, nv)).astype(np.float32) + 0.5).cuda()
+    funcs = (ramp_kernels.ramp_kernel_ramlak, ramp_kernels.hilbert_transform_kernel_halfoffset)
+    rf = RampFilterer(physpixwid=0.41, proj_2d_shape=(nu, nv), override_kern_funcs=funcs, apodization="hann")
+    outs = [torch.zeros_like(data) for _ in funcs] if layout != "strided" else None
+    outs = rf.filter(data, weights=w, scale=0.75, outs=outs)
+    d = data.cpu().numpy().astype(np.float64) * w.cpu().numpy().astype(np.float64)[None]
+    for taps, out in zip(rf.taps, outs):
+        want = 0.75 * np.stack([np.stack([conv_same_fp64(d[i, :, j], taps) for j in range(nv)], -1) for i in range(m)])
+        err = np.linalg.norm(out.cpu().numpy() - want) / np.linalg.norm(want)
+        assert err <= 1e-5, err
