@@ -157,6 +157,21 @@ def check(status: int, where: str) -> None:
     raise AprictError(status, where, detail)
 
 
+def upload(a: np.ndarray):  # noqa: ANN201
+    """A copy of host array ``a`` on the current CUDA device, enqueued on the
+    current stream without blocking the host.
+
+    A plain copy from pageable memory waits for the stream to drain first, so
+    the GPU would idle while the host prepares the next launch; here ``a`` is
+    staged in pinned memory (torch's caching host allocator holds the block
+    until the copy has run) and copied asynchronously. ``a`` may be changed
+    or freed as soon as this returns."""
+    import torch  # noqa: PLC0415
+
+    host = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return host.to(torch.device("cuda", torch.cuda.current_device()), non_blocking=True)
+
+
 def ptr(a: np.ndarray) -> ctypes.c_void_p:
     """Pointer to a numpy array's data (struct arguments are passed by
     pointer). The pointer object holds a reference to the array, so a

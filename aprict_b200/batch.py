@@ -51,7 +51,7 @@ class BatchPlan:
             lib.aprict_b200_batch_plan(op, _lib.ptr(scans), n, _lib.ptr(configs), self._host.ctypes.data, nbytes),
             "batch_plan",
         )
-        self._dev = torch.from_numpy(self._host.copy()).to(torch.device("cuda", torch.cuda.current_device()))
+        self._dev = _lib.upload(self._host)
         if self._dev.data_ptr() % 256:
             msg = "device plan is not 256-byte aligned"
             raise RuntimeError(msg)

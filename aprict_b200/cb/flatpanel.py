@@ -430,7 +430,8 @@ class ProjectionSet:
         """The packed views on the device (uint8 bytes, flattened), cached."""
         if self._specs_dev is None:
             raw = np.ascontiguousarray(self._proj_specs.reshape(-1)).view(np.uint8)
-            self._specs_dev = torch.from_numpy(raw.copy()).to(_device())
+            _device()
+            self._specs_dev = _lib.upload(raw)
         return self._specs_dev
 
     def create_buffer(self, *, dtype: type | np.dtype = np.float32, existing_ok: bool = False) -> None:

@@ -69,7 +69,7 @@ class RampFilterer:
                 raise ValueError(msg)
             self._taps_host.append(h)
             self._odd.append(ramp_kernels.odd_only(h))
-            self._taps.append(torch.from_numpy(h.astype(np.float32)).cuda())
+            self._taps.append(_lib.upload(h.astype(np.float32)))
         # Rows of 128 to 2048 samples are filtered by FFT from tables (kernel
         # spectrum and twiddles) built here once per filter, as the reference
         # keeps each filter's spectrum (ramp_filter.py:83-137); other lengths by
@@ -244,7 +244,7 @@ class FBPFilterer:
             apodization=apodization,
         )
         self._mask_host = frame_weight_mask(self._expanded_2d_shape, physpixwid, L, _hacky_fdk_mode)
-        self._mask = torch.from_numpy(self._mask_host).cuda()
+        self._mask = _lib.upload(self._mask_host)
         # Angle-0 fan/FDK path: the same weights folded into the convolution (FP32).
         nu, nv = self.proj_2d_shape
         u = physpixwid / L * (np.arange(nu, dtype=np.float64) - (nu - 1) / 2)
@@ -255,7 +255,7 @@ class FBPFilterer:
         else:
             w = 1.0 / (np.sqrt(1 + vv**2) ** 3 * np.sqrt(1 + vv**2 + uu**2))
         self._weights_host = w
-        self._weights = torch.from_numpy(w.astype(np.float32)).cuda()
+        self._weights = _lib.upload(w.astype(np.float32))
 
     # ---- the reference's helpers (ramp_filter.py:439-562) ----
 
@@ -386,11 +386,11 @@ class FBPFilterer:
         for a in range(0, n, per):
             b = min(n, a + per)
             ang = angles[a:b]
-            cs_fwd = torch.from_numpy(self._cs(-180 / np.pi * ang)).cuda()
-            cs_bwd = torch.from_numpy(self._cs(180 / np.pi * ang)).cuda()
+            cs_fwd = _lib.upload(self._cs(-180 / np.pi * ang))
+            cs_bwd = _lib.upload(self._cs(180 / np.pi * ang))
             colw = None
             if not hacky:
-                colw = torch.from_numpy(self._letterbox_matrix(ang)).cuda()
+                colw = _lib.upload(self._letterbox_matrix(ang))
             frame = torch.empty((b - a, nu_e, nv_e), dtype=torch.float32, device=data.device)
             src = data[a:b]
             d_src, d_frame = _desc(src), _desc(frame)  # kept alive across the calls
