@@ -2,8 +2,9 @@
 
 CPU tests pin the taps (src/aprict/ramp_kernels.py:43-59) against the
 known-answer vectors of src/aprict/tests/ramp_kernels/test_ramp_kernels_precision.py:33-147
-(extracted by tests/golden/make_ramp_golden.py). GPU tests compare the FP32
-shared-memory convolution kernel with an FP64 numpy convolution: gate rel L2
+(extracted by tests/golden/make_ramp_golden.py). GPU tests compare the filter
+kernels (the shared-memory FFT convolution for rows of 128 to 2048 samples, the
+direct convolution otherwise) with an FP64 numpy convolution: gate rel L2
 <= 1e-5, and the golden vectors within FP32 accuracy.
 """
 
