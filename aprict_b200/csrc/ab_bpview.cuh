@@ -82,7 +82,11 @@ struct ab_bpview_exact {
 
 // half_ext: the largest |x_i - c0_i| of any point the kernel projects
 // (voxel centres with sub-sample offsets), for the nearest-pixel thresholds.
-AB_HD bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, float sep, const double half_ext[3],
+// A call rather than inlined: it runs once per view and chunk in the
+// backprojectors, whose voxel loops then keep their accumulators in registers
+// (inlined, its FP64 temporaries made the fan-slice kernel spill 324 bytes
+// around the loop; out of line, 72 bytes).
+AB_HD_CALL bool ab_derive_bpview(const aprict_proj_spec &sp, ab_d3 c0, float voxwid, float sep, const double half_ext[3],
                             ab_bpview &o, ab_bpview_d *od = nullptr) {
     const ab_d3 s = ab_d3_of(sp.source_pos), P = ab_d3_of(sp.det_pos);
     const ab_d3 U = ab_d3_of(sp.det_u), V = ab_d3_of(sp.det_v);

@@ -16,9 +16,13 @@
 #if defined(__CUDACC__)
 #define AB_HD __host__ __device__ __forceinline__
 #define AB_DEV __device__ __forceinline__
+// a call, not inlined: for once-per-view set-up inside kernels whose hot loop
+// keeps many values in registers
+#define AB_HD_CALL __host__ __device__ inline __noinline__
 #else
 #define AB_HD inline
 #define AB_DEV inline
+#define AB_HD_CALL inline
 #endif
 
 // ---------------------------------------------------------------------------
