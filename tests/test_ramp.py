@@ -163,3 +163,44 @@ def test_gpu_filter_sizes_and_layouts(nu: int, layout: str) -> None:
         want = 0.75 * np.stack([np.stack([conv_same_fp64(d[i, :, j], taps) for j in range(nv)], -1) for i in range(m)])
         err = np.linalg.norm(out.cpu().numpy() - want) / np.linalg.norm(want)
         assert err <= 1e-5, err
+
+
+@pytest.mark.gpu
+def test_gpu_fft_entry_points_match_direct_through_the_c_abi() -> None:
+    """aprict_b200_ramp_fft_tables + aprict_b200_ramp_filter_fft against
+    aprict_b200_ramp_filter on the same rows, taps and weights, called through
+    ctypes as a C caller would: the tables built once, the filter run twice
+    (the tables are not consumed), rows along v with an odd row count."""
+    import torch
+
+    from aprict_b200 import _lib
+
+    lib = _lib.lib()
+    rng = np.random.default_rng(11)
+    m, nu, nv = 5, 700, 3  # 15 rows: the last complex signal carries one
+    x = torch.from_numpy(rng.random((m, nu, nv)).astype(np.float32)).cuda()
+    w = torch.from_numpy(rng.random((nu, nv)).astype(np.float32) + 0.5).cuda()
+    taps = torch.from_numpy(ramp_kernels.apodize_hann(ramp_kernels.ramp_kernel_ramlak(2 * nu - 1, 0.3)).astype(np.float32)).cuda()
+    nbytes = int(lib.aprict_b200_ramp_fft_tables_bytes(nu))
+    assert nbytes == 32 * 2048
+    tables = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.aprict_b200_ramp_fft_tables(taps.data_ptr(), nu, tables.data_ptr(), st), "ramp_fft_tables")
+    d = _lib.proj_desc(tuple(x.shape), tuple(x.stride()))
+    want = torch.empty_like(x)
+    _lib.check(
+        lib.aprict_b200_ramp_filter(_lib.ptr(d), x.data_ptr(), _lib.ptr(d), want.data_ptr(), taps.data_ptr(), 0,
+                                    w.data_ptr(), w.stride(0), w.stride(1), 0.25, st),
+        "ramp_filter",
+    )
+    for _ in range(2):
+        got = torch.full_like(x, float("nan"))
+        _lib.check(
+            lib.aprict_b200_ramp_filter_fft(_lib.ptr(d), x.data_ptr(), _lib.ptr(d), got.data_ptr(), tables.data_ptr(),
+                                            w.data_ptr(), w.stride(0), w.stride(1), 0.25, st),
+            "ramp_filter_fft",
+        )
+        torch.cuda.synchronize()
+        assert torch.isfinite(got).all()
+        err = (torch.linalg.norm((got - want).double()) / torch.linalg.norm(want.double())).item()
+        assert err <= 1e-5, err
